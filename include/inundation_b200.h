@@ -1,0 +1,185 @@
+/*
+ * inundation_b200: C ABI of the B200 shallow-water step.
+ *
+ * Plain C structs of device pointers and sizes; no allocation inside any entry
+ * point (the caller owns every buffer, sized by swe_workspace_bytes); every
+ * function enqueues on the given stream and returns a status code (0 = ok).
+ * Nothing is global, so calls on different streams with different buffers are
+ * independent.
+ *
+ * The entry points replace the device dispatches the reference records in
+ * inundation/vulkan/gpu_resident_batch.py. Each declaration names the
+ * reference kernel(s) or host call it stands for (file:line).
+ */
+#ifndef INUNDATION_B200_H
+#define INUNDATION_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *swe_stream_t; /* a cudaStream_t */
+
+enum swe_status {
+    SWE_OK = 0,
+    SWE_ERR_ARGUMENT = 1,     /* a null pointer, a zero size or an unknown mode */
+    SWE_ERR_CUDA = 2,         /* a CUDA launch or runtime call failed */
+    SWE_ERR_TOO_LARGE = 3,    /* a block's edge tile does not fit in shared memory */
+    SWE_ERR_MATH = 4,         /* the device arithmetic lost the two-sum error term */
+};
+
+/* Control block of the integer clock: 48 bytes, the layout of the reference's
+   RESIDENT_CTRL_DTYPE (inundation/vulkan/gpu_resident_batch.py:64-77). */
+typedef struct {
+    uint64_t now_ticks;
+    uint64_t stop_ticks;
+    uint64_t steps;
+    uint32_t dt_ticks;
+    uint32_t dt_max_ticks;
+    uint32_t dry_dt_ticks;
+    float last_raw;
+    float cfl_safety;
+    uint32_t pad;
+} swe_ctrl_t;
+
+/* Static mesh in the block-tile layout (device pointers).
+   Block b = cells [256 b, 256 b + 256). Its tile is the contiguous range
+   [tile_ptr[b], tile_ptr[b] + tile_count[b]) of the tile_* arrays: first the
+   edges whose left cell is in b (the reference's resident edge order,
+   gpu_resident_batch.py:175), then the edges whose right cell is in b and
+   left cell is not. lcsr[k] = (position in the tile << 1) | is_right for
+   the CSR slots k of each cell, in the reference's per-cell order
+   (inundation/mesh/geometry.py:454-468, remapped as blocks.py:33-44). */
+typedef struct {
+    uint32_t n_cells;
+    uint32_t n_blocks;
+    uint32_t max_tile_edges;  /* the largest tile_count */
+    uint32_t pad0;
+    const int32_t *tile_cl;   /* left cell */
+    const int32_t *tile_cr;   /* right cell, -1 on a wall */
+    const float *tile_nx;
+    const float *tile_ny;
+    const float *tile_len;
+    const float *tile_dzl;    /* face elevation minus the left bed */
+    const float *tile_dzr;
+    const uint32_t *tile_ptr;   /* n_blocks */
+    const uint32_t *tile_count; /* n_blocks */
+    const uint32_t *cptr;       /* n_cells + 1 */
+    const uint16_t *lcsr;       /* cptr[n_cells] */
+    const float *area;
+    const float *n_mann;
+    const uint32_t *ring_ptr;   /* block two-ring CSR (blocks.py:93-118) */
+    const uint32_t *ring_idx;
+} swe_mesh_t;
+
+/* Mutable state and the per-run workspace (device pointers). */
+typedef struct {
+    float *h, *hu, *hv, *h_lo;     /* committed state; h_lo: compensated low word */
+    float *h1, *hu1, *hv1, *h1_lo; /* Heun predictor */
+    float *clamp_mass;             /* per-cell positivity-clamp volume (diagnostic) */
+    uint32_t *blk;                 /* 3 words per block: wet, active, forced */
+    uint32_t *active_list;         /* n_blocks: active blocks of the current step */
+    uint32_t *sched;               /* 8 words: [0] active count, [1] next count, [2] done CTAs, [3] active blocks computed */
+    uint32_t *dt_buf;              /* [0] this step's dt (float bits, 0 = no-op), [1] next CFL bound */
+    swe_ctrl_t *ctrl;
+} swe_state_t;
+
+typedef struct {
+    float g;
+    float dry_tol;
+    float cfl;
+    uint32_t compensated; /* depth as a (h, h_lo) two-sum pair */
+    uint32_t track_clamp; /* accumulate the clamp diagnostic */
+    uint32_t active_set;  /* skip blocks outside the two-ring of wet blocks */
+    uint32_t grid;        /* CTAs of the persistent per-block kernels (0 = one per block) */
+    uint32_t pad;
+} swe_params_t;
+
+/* Sparse sources: n pairs (cell, dh/dt) on the device. */
+typedef struct {
+    const uint32_t *cells;
+    const float *rate;
+    uint32_t count;
+    uint32_t pad;
+} swe_sources_t;
+
+/* Bytes of device workspace: active list + sched words + dt words (+ volume partials). */
+size_t swe_workspace_bytes(uint32_t n_cells);
+
+/* Dynamic shared memory one per-block CTA needs for a tile of max_tile_edges. */
+size_t swe_tile_smem_bytes(uint32_t max_tile_edges);
+
+/* Persistent CTAs per SM for the per-block kernels at that tile size (occupancy query). */
+int swe_blocks_per_sm(uint32_t max_tile_edges, int *out);
+
+/* One Heun stage over the active blocks, fused: edge fluxes of each block's
+   tile into shared memory, the fixed-order per-cell gather and the update.
+   stage 0 = predictor, 1 = corrector (adds the next step's CFL bound and the
+   wet marks). Replaces flux_resident_gather + update_resident_gather[_comp]
+   (inundation/vulkan/shaders/resident.py:187-291 and 401-513). */
+int swe_stage(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params_t *params, int stage,
+              swe_stream_t stream);
+
+/* Sparse sources after the Heun step: compensated add, wet marks, then the
+   post-source CFL bound of each wet source cell. Replaces source_resident
+   (resident.py:665-733). */
+int swe_apply_sources(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params_t *params,
+                      const swe_sources_t *sources, swe_stream_t stream);
+
+/* Active flags = (wet | forced) dilated over each block's two-ring, compacted
+   into active_list; then, when control_mode >= 0, step_control in the last
+   CTA. force = 1 also on a no-op step. Replaces block_dilate + step_control
+   (resident.py:778-805, 813-885). */
+int swe_block_dilate_compact(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params_t *params,
+                             int force, int control_mode, swe_stream_t stream);
+
+/* Start of a run: wet flag of every block from the state (or all active).
+   Replaces block_mark (resident.py:738-773). */
+int swe_block_mark(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params_t *params,
+                   swe_stream_t stream);
+
+/* Prologue CFL bound of the current state into dt_buf[0] (reset to 1e30
+   first). Replaces dt_reset + cfl_edge_gather + cfl_gather
+   (cfl.py:130-166, resident.py:528-610). */
+int swe_cfl_prologue(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params_t *params,
+                     swe_stream_t stream);
+
+/* Integer-tick step control; mode 0 START, 1 STEP, 2 RETARGET.
+   Replaces step_control (resident.py:813-885). */
+int swe_step_control(swe_ctrl_t *ctrl, uint32_t *dt_buf, int mode, swe_stream_t stream);
+
+/* Whole prologue: block_mark, forced dilation, CFL bound, START
+   (gpu_resident_batch.py:567-591). */
+int swe_prologue(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params_t *params,
+                 swe_stream_t stream);
+
+/* One whole step: two stages, sources (if any), dilation and STEP control
+   (gpu_resident_batch.py:489-513). */
+int swe_step(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params_t *params,
+             const swe_sources_t *sources, swe_stream_t stream);
+
+/* Sum of (h + h_lo) * area in float64, in a fixed order: partials holds
+   swe_volume_partials(n) doubles. The reference does this on the host
+   (inundation/workflow.py:913-922). */
+uint32_t swe_volume_partials(uint32_t n_cells);
+int swe_volume_fp64(const float *h, const float *h_lo, const float *area, uint32_t n_cells, double *partials,
+                    double *out, swe_stream_t stream);
+
+/* The two-sum of (v[0], v[1]) into v[2] (its error term) on the device: the
+   reference's fast-math guard (inundation/vulkan/solver.py:449-467,
+   resident.py:889-907). */
+int swe_eft_probe(float *v, swe_stream_t stream);
+
+/* (x^(4/3)) of n values on the device, the Manning depth power the update uses. */
+int swe_pow43(const float *x, float *out, uint32_t n, swe_stream_t stream);
+
+const char *swe_status_string(int status);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* INUNDATION_B200_H */

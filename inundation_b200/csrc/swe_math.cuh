@@ -1,0 +1,157 @@
+// Device arithmetic of the shallow-water step, in float32.
+//
+// Each function evaluates the same expression, in the same order, as the
+// reference's GLSL (inundation/vulkan/shaders/flux.py:43-182 and 301-319), so
+// that with contraction off (--fmad=false) and IEEE division and square root
+// every result is reproducible bit for bit. GLSL min/max/clamp are written
+// with their specified comparisons: min(x,y) = y<x ? y : x, max(x,y) = x<y ? y : x.
+#pragma once
+#include <cstdint>
+
+namespace swe {
+
+constexpr float kFilmDepths = 4.0f;
+constexpr float kTicksPerSecond = 1048576.0f;
+constexpr float kDtSentinel = 1e30f;
+
+struct Phys {
+    float g;
+    float dry_tol;
+};
+
+__device__ __forceinline__ float gmin(float x, float y) { return (y < x) ? y : x; }
+__device__ __forceinline__ float gmax(float x, float y) { return (x < y) ? y : x; }
+__device__ __forceinline__ float gclamp(float x, float lo, float hi) { return gmin(gmax(x, lo), hi); }
+
+// x^(4/3) for x > 0: cube root by Newton's iteration r <- (2r + x/r^2)/3
+// from the exponent-thirds estimate bits(x)/3 + (2/3)*127*2^23, then x*r.
+// Basic IEEE operations only, so host and device agree exactly.
+__device__ __forceinline__ float pow43(float x) {
+    float r = __uint_as_float(__float_as_uint(x) / 3u + 0x2A555555u);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) r = (2.0f * r + x / (r * r)) / 3.0f;
+    return x * r;
+}
+
+// Desingularised velocity (Kurganov & Petrova 2007): hq/h above the film depth.
+__device__ __forceinline__ float safe_vel(const Phys &p, float h, float hq) {
+    const float e = kFilmDepths * p.dry_tol;
+    return (h > p.dry_tol) ? 2.0f * h * hq / (h * h + gmax(h * h, e * e)) : 0.0f;
+}
+
+// HLLC wave-speed bounds: Roe average, blended continuously into Toro's
+// dry-bed speeds u -+ 2c as a side goes from one to two dry_tol deep.
+__device__ __forceinline__ void hllc_speeds(const Phys &p, float hL, float unL, float hR, float unR, float &SLo,
+                                            float &SRo) {
+    const float cL = sqrtf(p.g * gmax(hL, 0.0f));
+    const float cR = sqrtf(p.g * gmax(hR, 0.0f));
+    const float sqL = sqrtf(gmax(hL, 0.0f));
+    const float sqR = sqrtf(gmax(hR, 0.0f));
+    const float den = sqL + sqR;
+    const float u_roe = (den > 1e-12f) ? (sqL * unL + sqR * unR) / den : 0.0f;
+    const float c_roe = sqrtf(p.g * 0.5f * (hL + hR));
+    const float SL = gmin(unL - cL, u_roe - c_roe);
+    const float SR = gmax(unR + cR, u_roe + c_roe);
+    const float wetL = gclamp(hL / p.dry_tol - 1.0f, 0.0f, 1.0f);
+    const float wetR = gclamp(hR / p.dry_tol - 1.0f, 0.0f, 1.0f);
+    const float dryLeft = (1.0f - wetL) * wetR;
+    const float dryRight = (1.0f - wetR) * wetL;
+    const float roe = 1.0f - dryLeft - dryRight;
+    SLo = roe * SL + dryLeft * (unR - 2.0f * cR) + dryRight * (unL - cL);
+    SRo = roe * SR + dryLeft * (unR + cR) + dryRight * (unL + 2.0f * cL);
+}
+
+// HLLC flux in the face frame (Toro 2001); smax is the largest speed assumed.
+__device__ __forceinline__ void hllc(const Phys &p, float hL, float hqnL, float hqtL, float hR, float hqnR,
+                                     float hqtR, float &Fh, float &Fhn, float &Fht, float &smax) {
+    const float unL = safe_vel(p, hL, hqnL), utL = safe_vel(p, hL, hqtL);
+    const float unR = safe_vel(p, hR, hqnR), utR = safe_vel(p, hR, hqtR);
+    float SL, SR;
+    hllc_speeds(p, hL, unL, hR, unR, SL, SR);
+    smax = gmax(fabsf(SL), fabsf(SR));
+    const float num_sm = SL * hR * (unR - SR) - SR * hL * (unL - SL);
+    const float den_sm = hR * (unR - SR) - hL * (unL - SL);
+    const float SM = (fabsf(den_sm) > 1e-12f) ? num_sm / den_sm : 0.0f;
+    if (SL >= 0.0f) {
+        Fh = hL * unL;
+        Fhn = hL * unL * unL + 0.5f * p.g * hL * hL;
+        Fht = hL * unL * utL;
+    } else if (SM >= 0.0f) {
+        const float dSL = SL - SM;
+        const float kL = hL * (SL - unL) / ((fabsf(dSL) > 1e-14f) ? dSL : 1e-14f);
+        Fh = hL * unL + SL * (kL - hL);
+        Fhn = (hL * unL * unL + 0.5f * p.g * hL * hL) + SL * (kL * SM - hL * unL);
+        Fht = hL * unL * utL + SL * (kL * utL - hL * utL);
+    } else if (SR >= 0.0f) {
+        const float dSR = SR - SM;
+        const float kR = hR * (SR - unR) / ((fabsf(dSR) > 1e-14f) ? dSR : 1e-14f);
+        Fh = hR * unR + SR * (kR - hR);
+        Fhn = (hR * unR * unR + 0.5f * p.g * hR * hR) + SR * (kR * SM - hR * unR);
+        Fht = hR * unR * utR + SR * (kR * utR - hR * utR);
+    } else {
+        Fh = hR * unR;
+        Fhn = hR * unR * unR + 0.5f * p.g * hR * hR;
+        Fht = hR * unR * utR;
+    }
+}
+
+// Audusse hydrostatic reconstruction: depths at the face elevation, momenta
+// rebuilt from the cells' velocities, rotated into the face frame.
+__device__ __forceinline__ void face_states(const Phys &p, float hL, float huL, float hvL, float dzL, float hR,
+                                            float huR, float hvR, float dzR, float nx, float ny, float &hLs,
+                                            float &hqnL, float &hqtL, float &hRs, float &hqnR, float &hqtR) {
+    hLs = gmax(0.0f, hL - dzL);
+    hRs = gmax(0.0f, hR - dzR);
+    const float uL = safe_vel(p, hL, huL), vL = safe_vel(p, hL, hvL);
+    const float uR = safe_vel(p, hR, huR), vR = safe_vel(p, hR, hvR);
+    const float huLs = hLs * uL, hvLs = hLs * vL, huRs = hRs * uR, hvRs = hRs * vR;
+    hqnL = huLs * nx + hvLs * ny;
+    hqtL = -huLs * ny + hvLs * nx;
+    hqnR = huRs * nx + hvRs * ny;
+    hqtR = -huRs * ny + hvRs * nx;
+}
+
+// The CFL wave speed the flux would assume on an edge.
+__device__ __forceinline__ float wave_bound(const Phys &p, float hL, float huL, float hvL, float dzL, float hR,
+                                            float huR, float hvR, float dzR, float nx, float ny) {
+    float hLs, hqnL, hqtL, hRs, hqnR, hqtR, SL, SR;
+    face_states(p, hL, huL, hvL, dzL, hR, huR, hvR, dzR, nx, ny, hLs, hqnL, hqtL, hRs, hqnR, hqtR);
+    hllc_speeds(p, hLs, safe_vel(p, hLs, hqnL), hRs, safe_vel(p, hRs, hqnR), SL, SR);
+    return gmax(fabsf(SL), fabsf(SR));
+}
+
+// Wall ghost: the left state mirrored in the normal direction.
+__device__ __forceinline__ void wall_mirror(float huL, float hvL, float nx, float ny, float &huR, float &hvR) {
+    huR = huL - 2.0f * (huL * nx + hvL * ny) * nx;
+    hvR = hvL - 2.0f * (huL * nx + hvL * ny) * ny;
+}
+
+// Semi-implicit momentum decay factor of a thin film (a rate, independent of the tick).
+__device__ __forceinline__ float film_drag(const Phys &p, float h, float dt) {
+    const float e = kFilmDepths * p.dry_tol;
+    if (h >= e) return 1.0f;
+    const float rate = (e * e - h * h) / (2.0f * h * h) * sqrtf(p.g / e);
+    return 1.0f / (1.0f + dt * rate);
+}
+
+// Knuth's two-sum: s + e == a + b exactly.
+__device__ __forceinline__ void two_sum(float a, float b, float &s, float &e) {
+    const float t = a + b;
+    const float bb = t - a;
+    e = (a - (t - bb)) + (b - bb);
+    s = t;
+}
+
+// (hi + lo) + inc as a renormalised pair, clamped at zero.
+__device__ __forceinline__ void add_compensated(float hi, float lo, float inc, float &h_new, float &lo_new) {
+    float s, e;
+    two_sum(hi, inc, s, e);
+    e += lo;
+    two_sum(s, e, h_new, lo_new);
+    if (h_new < 0.0f || (h_new == 0.0f && lo_new < 0.0f)) {
+        h_new = 0.0f;
+        lo_new = 0.0f;
+    }
+}
+
+}  // namespace swe

@@ -1,0 +1,116 @@
+"""ctypes binding of ``lib/libinundation_b200.so`` (the C ABI in ``include/inundation_b200.h``).
+
+The library is the only compute path: if it is missing or cannot be loaded,
+``load()`` raises. There is no CPU fallback.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+from .build import LIB_PATH
+
+_P = ctypes.c_void_p
+_U32 = ctypes.c_uint32
+
+STATUS_MESSAGES = {
+    1: "invalid argument",
+    2: "CUDA launch or runtime error",
+    3: "a block's edge tile does not fit in shared memory",
+    4: "device arithmetic lost the two-sum error term",
+}
+
+# Every function the header declares, with its argument and result types.
+_SIGNATURES: dict[str, tuple[list, object]] = {
+    "swe_workspace_bytes": ([_U32], ctypes.c_size_t),
+    "swe_tile_smem_bytes": ([_U32], ctypes.c_size_t),
+    "swe_blocks_per_sm": ([_U32, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "swe_stage": ([_P, _P, _P, ctypes.c_int, _P], ctypes.c_int),
+    "swe_apply_sources": ([_P, _P, _P, _P, _P], ctypes.c_int),
+    "swe_block_dilate_compact": ([_P, _P, _P, ctypes.c_int, ctypes.c_int, _P], ctypes.c_int),
+    "swe_block_mark": ([_P, _P, _P, _P], ctypes.c_int),
+    "swe_cfl_prologue": ([_P, _P, _P, _P], ctypes.c_int),
+    "swe_step_control": ([_P, _P, ctypes.c_int, _P], ctypes.c_int),
+    "swe_prologue": ([_P, _P, _P, _P], ctypes.c_int),
+    "swe_step": ([_P, _P, _P, _P, _P], ctypes.c_int),
+    "swe_volume_partials": ([_U32], _U32),
+    "swe_volume_fp64": ([_P, _P, _P, _U32, _P, _P, _P], ctypes.c_int),
+    "swe_eft_probe": ([_P, _P], ctypes.c_int),
+    "swe_pow43": ([_P, _P, _U32, _P], ctypes.c_int),
+    "swe_status_string": ([ctypes.c_int], ctypes.c_char_p),
+}
+
+
+class SweMesh(ctypes.Structure):
+    _fields_ = [
+        ("n_cells", _U32),
+        ("n_blocks", _U32),
+        ("max_tile_edges", _U32),
+        ("pad0", _U32),
+        *[(name, _P) for name in (
+            "tile_cl", "tile_cr", "tile_nx", "tile_ny", "tile_len", "tile_dzl", "tile_dzr", "tile_ptr",
+            "tile_count", "cptr", "lcsr", "area", "n_mann", "ring_ptr", "ring_idx",
+        )],
+    ]
+
+
+class SweState(ctypes.Structure):
+    _fields_ = [
+        (name, _P)
+        for name in (
+            "h", "hu", "hv", "h_lo", "h1", "hu1", "hv1", "h1_lo", "clamp_mass", "blk", "active_list", "sched",
+            "dt_buf", "ctrl",
+        )
+    ]
+
+
+class SweParams(ctypes.Structure):
+    _fields_ = [
+        ("g", ctypes.c_float),
+        ("dry_tol", ctypes.c_float),
+        ("cfl", ctypes.c_float),
+        ("compensated", _U32),
+        ("track_clamp", _U32),
+        ("active_set", _U32),
+        ("grid", _U32),
+        ("pad", _U32),
+    ]
+
+
+class SweSources(ctypes.Structure):
+    _fields_ = [("cells", _P), ("rate", _P), ("count", _U32), ("pad", _U32)]
+
+
+_LIB: ctypes.CDLL | None = None
+
+
+def library_path() -> Path:
+    return LIB_PATH
+
+
+def load() -> ctypes.CDLL:
+    """Load the CUDA library (raises if it was not built)."""
+    global _LIB
+    if _LIB is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(
+                f"CUDA extension {LIB_PATH} is missing: build it with `python -m inundation_b200.build`"
+            )
+        lib = ctypes.CDLL(str(LIB_PATH))
+        for name, (args, res) in _SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = res
+        _LIB = lib
+    return _LIB
+
+
+def check(rc: int, what: str) -> None:
+    """Turn a status code into an exception (0 is success)."""
+    if rc != 0:
+        raise RuntimeError(f"{what} failed: {STATUS_MESSAGES.get(rc, f'status {rc}')}")
+
+
+def exported_symbols() -> list[str]:
+    return list(_SIGNATURES)

@@ -1,0 +1,485 @@
+/*
+ * FP32 oracle of the reference's GPU-resident shallow-water kernels.
+ * TEST INFRASTRUCTURE ONLY: the checker, never the product. Only tests/,
+ * __graft_entry__.smoke() and bench.py's CPU-baseline arm load it.
+ *
+ * A literal, sequential C restatement of the GLSL compute kernels of the
+ * reference's resident backend, on the reference's own data layout (edges
+ * sorted by the block of their left cell, a 6-word per-edge flux buffer, the
+ * remapped signed CSR, per-block flag words {wet, active, forced}):
+ *
+ *   safe_vel, hllc_speeds, hllc, face_states, wave_bound
+ *       inundation/vulkan/shaders/flux.py:63-182
+ *   film_drag                      flux.py:46-51
+ *   two_sum, add_compensated       flux.py:301-319
+ *   flux_resident_gather           resident.py:187-291 (wall ghost :125-146, words :165-184)
+ *   update_resident_gather[_comp]  resident.py:401-513 (sum :312-344, depth :359-398)
+ *   source_resident                resident.py:665-730
+ *   block_mark, block_dilate       resident.py:738-802
+ *   cfl_edge_gather, cfl_gather    resident.py:528-607
+ *   step_control                   resident.py:813-882
+ *
+ * Every expression keeps the GLSL evaluation order; it is compiled with
+ * -ffp-contract=off so no multiply-add is fused. GLSL min/max/clamp are
+ * spelled out with their specified comparisons (min(x,y) = y<x ? y : x,
+ * max(x,y) = x<y ? y : x). GLSL's pow has no fixed rounding, so
+ * pow(h, 4/3) is evaluated by the same cube-root Newton sequence as the CUDA
+ * kernels (pow43 below): a value the reference admits, bit-identical to the
+ * product's.
+ *
+ * One deliberate choice: the GLSL source kernel reads a neighbour's depth
+ * while that neighbour's own source may be adding to it (a race in the
+ * reference). Here all sources are added first and the post-source bounds
+ * are taken after, which is one of the outcomes the reference allows.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#define EF_WORDS 6u
+#define EF_CFL 5u
+#define BLK_WORDS 3u
+#define BLK_WET 0u
+#define BLK_ACTIVE 1u
+#define BLK_FORCED 2u
+#define FILM_DEPTHS 4.0f
+#define TICKS_PER_SECOND 1048576.0f
+#define DT_SENTINEL 1e30f
+
+typedef struct {
+    uint64_t now_ticks;
+    uint64_t stop_ticks;
+    uint64_t steps;
+    uint32_t dt_ticks;
+    uint32_t dt_max_ticks;
+    uint32_t dry_dt_ticks;
+    float last_raw;
+    float cfl_safety;
+    uint32_t pad;
+} ctrl_t;
+
+/* Everything one resident solver holds, in the reference's layout. */
+typedef struct {
+    uint32_t N, E, n_blocks;
+    float g, dry_tol, cfl;
+    const int32_t *ecL, *ecR;
+    const float *enx, *eny, *elen, *edz; /* edz: (dzL, dzR) pairs */
+    const float *area, *n_mann;
+    const uint32_t *cptr, *cidx;
+    const uint32_t *erange; /* (first, last) left-cell block per 256-edge workgroup */
+    const uint32_t *bptr, *bidx; /* block two-ring */
+    float *h, *hu, *hv, *h1, *hu1, *hv1, *h_lo, *h1_lo;
+    float *ef;
+    uint32_t *touched;
+    uint32_t *blk;
+    uint32_t *dt_buf; /* [0] this step's dt bits, [1] next step's CFL bound bits */
+    float *clamp_mass;
+    ctrl_t *ctrl;
+} oracle_t;
+
+static inline uint32_t fbits(float f) { uint32_t u; memcpy(&u, &f, 4); return u; }
+static inline float bitsf(uint32_t u) { float f; memcpy(&f, &u, 4); return f; }
+static inline float gmin(float x, float y) { return (y < x) ? y : x; }
+static inline float gmax(float x, float y) { return (x < y) ? y : x; }
+static inline float gclamp(float x, float lo, float hi) { return gmin(gmax(x, lo), hi); }
+
+/* x^(1/3) for x > 0 by Newton's iteration r <- (2r + x/r^2)/3 from the
+   bit-level estimate bits(x)/3 + (2/3)*127*2^23 (the exponent divided by
+   three), then x * r. Basic IEEE operations only. */
+static float pow43(float x) {
+    uint32_t i = fbits(x);
+    float r = bitsf(i / 3u + 0x2A555555u);
+    for (int k = 0; k < 4; ++k) r = (2.0f * r + x / (r * r)) / 3.0f;
+    return x * r;
+}
+
+static float safe_vel(const oracle_t *o, float h_, float hq) {
+    float e_ = FILM_DEPTHS * o->dry_tol;
+    return (h_ > o->dry_tol) ? 2.0f * h_ * hq / (h_ * h_ + gmax(h_ * h_, e_ * e_)) : 0.0f;
+}
+
+static void hllc_speeds(const oracle_t *o, float hL, float unL, float hR, float unR, float *SLo, float *SRo) {
+    float g = o->g;
+    float cL = sqrtf(g * gmax(hL, 0.0f));
+    float cR = sqrtf(g * gmax(hR, 0.0f));
+    float sqL = sqrtf(gmax(hL, 0.0f));
+    float sqR = sqrtf(gmax(hR, 0.0f));
+    float den = sqL + sqR;
+    float u_roe = (den > 1e-12f) ? (sqL * unL + sqR * unR) / den : 0.0f;
+    float c_roe = sqrtf(g * 0.5f * (hL + hR));
+    float SL = gmin(unL - cL, u_roe - c_roe);
+    float SR = gmax(unR + cR, u_roe + c_roe);
+    float wetL = gclamp(hL / o->dry_tol - 1.0f, 0.0f, 1.0f);
+    float wetR = gclamp(hR / o->dry_tol - 1.0f, 0.0f, 1.0f);
+    float dryLeft = (1.0f - wetL) * wetR;
+    float dryRight = (1.0f - wetR) * wetL;
+    float roe = 1.0f - dryLeft - dryRight;
+    *SLo = roe * SL + dryLeft * (unR - 2.0f * cR) + dryRight * (unL - cL);
+    *SRo = roe * SR + dryLeft * (unR + cR) + dryRight * (unL + 2.0f * cL);
+}
+
+static void hllc(const oracle_t *o, float hL, float hqnL, float hqtL, float hR, float hqnR, float hqtR,
+                 float *Fh, float *Fhn, float *Fht, float *Smax) {
+    float g = o->g;
+    float unL = safe_vel(o, hL, hqnL), utL = safe_vel(o, hL, hqtL);
+    float unR = safe_vel(o, hR, hqnR), utR = safe_vel(o, hR, hqtR);
+    float SL, SR;
+    hllc_speeds(o, hL, unL, hR, unR, &SL, &SR);
+    *Smax = gmax(fabsf(SL), fabsf(SR));
+    float num_sm = SL * hR * (unR - SR) - SR * hL * (unL - SL);
+    float den_sm = hR * (unR - SR) - hL * (unL - SL);
+    float SM = (fabsf(den_sm) > 1e-12f) ? num_sm / den_sm : 0.0f;
+    float FL_h = hL * unL;
+    float FL_hn = hL * unL * unL + 0.5f * g * hL * hL;
+    float FL_ht = hL * unL * utL;
+    float FR_h = hR * unR;
+    float FR_hn = hR * unR * unR + 0.5f * g * hR * hR;
+    float FR_ht = hR * unR * utR;
+    float dSL = SL - SM, dSR = SR - SM;
+    float kL = hL * (SL - unL) / ((fabsf(dSL) > 1e-14f) ? dSL : 1e-14f);
+    float kR = hR * (SR - unR) / ((fabsf(dSR) > 1e-14f) ? dSR : 1e-14f);
+    float FsL_h = FL_h + SL * (kL - hL);
+    float FsL_hn = FL_hn + SL * (kL * SM - hL * unL);
+    float FsL_ht = FL_ht + SL * (kL * utL - hL * utL);
+    float FsR_h = FR_h + SR * (kR - hR);
+    float FsR_hn = FR_hn + SR * (kR * SM - hR * unR);
+    float FsR_ht = FR_ht + SR * (kR * utR - hR * utR);
+    if (SL >= 0.0f) { *Fh = FL_h; *Fhn = FL_hn; *Fht = FL_ht; }
+    else if (SM >= 0.0f) { *Fh = FsL_h; *Fhn = FsL_hn; *Fht = FsL_ht; }
+    else if (SR >= 0.0f) { *Fh = FsR_h; *Fhn = FsR_hn; *Fht = FsR_ht; }
+    else { *Fh = FR_h; *Fhn = FR_hn; *Fht = FR_ht; }
+}
+
+static void face_states(const oracle_t *o, float hL, float huL, float hvL, float dzL, float hR, float huR,
+                        float hvR, float dzR, float nx_, float ny_, float *hLs, float *hqnL, float *hqtL,
+                        float *hRs, float *hqnR, float *hqtR) {
+    *hLs = gmax(0.0f, hL - dzL);
+    *hRs = gmax(0.0f, hR - dzR);
+    float uL = safe_vel(o, hL, huL), vL = safe_vel(o, hL, hvL);
+    float uR = safe_vel(o, hR, huR), vR = safe_vel(o, hR, hvR);
+    float huLs = *hLs * uL, hvLs = *hLs * vL, huRs = *hRs * uR, hvRs = *hRs * vR;
+    *hqnL = huLs * nx_ + hvLs * ny_;
+    *hqtL = -huLs * ny_ + hvLs * nx_;
+    *hqnR = huRs * nx_ + hvRs * ny_;
+    *hqtR = -huRs * ny_ + hvRs * nx_;
+}
+
+static float wave_bound(const oracle_t *o, float hL, float huL, float hvL, float dzL, float hR, float huR,
+                        float hvR, float dzR, float nx_, float ny_) {
+    float hLs, hqnL, hqtL, hRs, hqnR, hqtR, SL, SR;
+    face_states(o, hL, huL, hvL, dzL, hR, huR, hvR, dzR, nx_, ny_, &hLs, &hqnL, &hqtL, &hRs, &hqnR, &hqtR);
+    hllc_speeds(o, hLs, safe_vel(o, hLs, hqnL), hRs, safe_vel(o, hRs, hqnR), &SL, &SR);
+    return gmax(fabsf(SL), fabsf(SR));
+}
+
+static float film_drag(const oracle_t *o, float h_, float dt_) {
+    float e_ = FILM_DEPTHS * o->dry_tol;
+    if (h_ >= e_) return 1.0f;
+    float rate = (e_ * e_ - h_ * h_) / (2.0f * h_ * h_) * sqrtf(o->g / e_);
+    return 1.0f / (1.0f + dt_ * rate);
+}
+
+static void two_sum(float a, float b, float *s, float *e) {
+    float t = a + b;
+    float bb = t - a;
+    float err = (a - (t - bb)) + (b - bb);
+    *s = t;
+    *e = err;
+}
+
+static void add_compensated(float hi, float loi, float inc, float *h_new, float *lo_new) {
+    float s, e;
+    two_sum(hi, inc, &s, &e);
+    e += loi;
+    two_sum(s, e, h_new, lo_new);
+    if (*h_new < 0.0f || (*h_new == 0.0f && *lo_new < 0.0f)) { *h_new = 0.0f; *lo_new = 0.0f; }
+}
+
+static inline int block_active(const oracle_t *o, uint32_t b) { return o->blk[BLK_WORDS * b + BLK_ACTIVE] != 0u; }
+
+static void load_state(const oracle_t *o, int stage, int c, float *h_, float *hu_, float *hv_) {
+    if (stage && block_active(o, (uint32_t)c >> 8)) { *h_ = o->h1[c]; *hu_ = o->hu1[c]; *hv_ = o->hv1[c]; }
+    else { *h_ = o->h[c]; *hu_ = o->hu[c]; *hv_ = o->hv[c]; }
+}
+
+void oracle_flux_stage(oracle_t *o, int stage) {
+    if (o->dt_buf[0] == 0u) return;
+    uint32_t n_wg = (o->E + 255u) / 256u;
+    for (uint32_t wg = 0; wg < n_wg; ++wg) {
+        int live = 0;
+        for (uint32_t b = o->erange[2u * wg]; b <= o->erange[2u * wg + 1u]; ++b)
+            if (block_active(o, b)) { live = 1; break; }
+        if (!live) continue;
+        uint32_t e_end = (wg + 1u) * 256u < o->E ? (wg + 1u) * 256u : o->E;
+        for (uint32_t eid = wg * 256u; eid < e_end; ++eid) {
+            int cL = o->ecL[eid], cR = o->ecR[eid];
+            float nx_ = o->enx[eid], ny_ = o->eny[eid], len = o->elen[eid];
+            float hL, huL, hvL, hR, huR, hvR;
+            load_state(o, stage, cL, &hL, &huL, &hvL);
+            if (cR == -1) {
+                hR = hL;
+                huR = huL - 2.0f * (huL * nx_ + hvL * ny_) * nx_;
+                hvR = hvL - 2.0f * (huL * nx_ + hvL * ny_) * ny_;
+            } else {
+                load_state(o, stage, cR, &hR, &huR, &hvR);
+            }
+            if (hL < o->dry_tol && hR < o->dry_tol) continue;
+            float dzL = o->edz[2u * eid], dzR = o->edz[2u * eid + 1u];
+            float hLs, hqnL, hqtL, hRs, hqnR, hqtR, Fh, Fhn, Fht, Smax;
+            face_states(o, hL, huL, hvL, dzL, hR, huR, hvR, dzR, nx_, ny_, &hLs, &hqnL, &hqtL, &hRs, &hqnR, &hqtR);
+            hllc(o, hLs, hqnL, hqtL, hRs, hqnR, hqtR, &Fh, &Fhn, &Fht, &Smax);
+            if (cR < 0) Fh = 0.0f; /* a wall passes no mass */
+            float Fhu = Fhn * nx_ - Fht * ny_;
+            float Fhv = Fhn * ny_ + Fht * nx_;
+            float SL_g = 0.5f * o->g * (hL * hL - hLs * hLs);
+            float SR_g = 0.5f * o->g * (hR * hR - hRs * hRs);
+            o->touched[cL] = 1u;
+            if (cR >= 0) o->touched[cR] = 1u;
+            float *w = o->ef + EF_WORDS * eid;
+            w[0] = Fh * len;
+            w[1] = Fhu * len + SL_g * nx_ * len;
+            w[2] = Fhv * len + SL_g * ny_ * len;
+            w[3] = Fhu * len + SR_g * nx_ * len;
+            w[4] = Fhv * len + SR_g * ny_ * len;
+            if (stage) w[EF_CFL] = Smax * len;
+        }
+    }
+}
+
+void oracle_update_stage(oracle_t *o, int stage, int compensated, int track_clamp) {
+    if (o->dt_buf[0] == 0u) return;
+    for (uint32_t i = 0; i < o->N; ++i) {
+        uint32_t b = i >> 8;
+        if (!block_active(o, b)) continue;
+        if (!stage && (i & 255u) == 0u) o->blk[BLK_WORDS * b + BLK_WET] = 0u;
+        float A = o->area[i];
+        float dt = bitsf(o->dt_buf[0]);
+        float dti = dt / A;
+        float hi, hui, hvi;
+        if (!stage) { hi = o->h[i]; hui = o->hu[i]; hvi = o->hv[i]; }
+        else { hi = o->h1[i]; hui = o->hu1[i]; hvi = o->hv1[i]; }
+        float sdh = 0.0f, sdhu = 0.0f, sdhv = 0.0f, lam = 0.0f;
+        uint32_t kend = o->cptr[i];
+        if (o->touched[i] != 0u) { o->touched[i] = 0u; kend = o->cptr[i + 1u]; }
+        int own_dry = hi < o->dry_tol;
+        for (uint32_t k = o->cptr[i]; k < kend; ++k) {
+            uint32_t s = o->cidx[k], e = s >> 1;
+            int right = (s & 1u) != 0u;
+            if (own_dry) {
+                int nb = right ? o->ecL[e] : o->ecR[e];
+                if (nb == -1) continue;
+                if (nb >= 0) {
+                    int pred = stage && block_active(o, (uint32_t)nb >> 8);
+                    if ((pred ? o->h1[nb] : o->h[nb]) < o->dry_tol) continue;
+                }
+            }
+            const float *w = o->ef + EF_WORDS * e;
+            if (right) { sdh -= w[0]; sdhu -= w[3]; sdhv -= w[4]; }
+            else { sdh += w[0]; sdhu += w[1]; sdhv += w[2]; }
+            if (stage) lam += w[EF_CFL];
+        }
+        float h_new, lo_new, h_raw;
+        if (compensated) {
+            float loi = !stage ? o->h_lo[i] : o->h1_lo[i];
+            add_compensated(hi, loi, -dti * sdh, &h_new, &lo_new);
+            float s_raw, e_raw;
+            two_sum(hi, -dti * sdh, &s_raw, &e_raw);
+            h_raw = s_raw + (e_raw + loi);
+        } else {
+            h_raw = hi - dti * sdh;
+            h_new = gmax(h_raw, 0.0f);
+            lo_new = 0.0f;
+        }
+        float hu_new = hui - dti * sdhu;
+        float hv_new = hvi - dti * sdhv;
+        if (track_clamp) o->clamp_mass[i] += 0.5f * A * (h_new - h_raw);
+        if (h_new < o->dry_tol) { hu_new = 0.0f; hv_new = 0.0f; }
+        if (h_new >= o->dry_tol) {
+            float drag = film_drag(o, h_new, dt);
+            hu_new *= drag;
+            hv_new *= drag;
+        }
+        if (h_new >= o->dry_tol) {
+            float n = o->n_mann[i];
+            float u_ = hu_new / h_new, v_ = hv_new / h_new;
+            float spd = sqrtf(u_ * u_ + v_ * v_);
+            float h43 = pow43(h_new);
+            float Sf = o->g * n * n * spd / h43;
+            float den = 1.0f + dt * Sf;
+            hu_new = hu_new / den;
+            hv_new = hv_new / den;
+        }
+        float hf = 0.0f;
+        if (compensated) {
+            if (!stage) { o->h1[i] = h_new; o->h1_lo[i] = lo_new; }
+            else {
+                float s, e, lof;
+                two_sum(o->h[i], h_new, &s, &e);
+                e += o->h_lo[i] + lo_new;
+                two_sum(0.5f * s, 0.5f * e, &hf, &lof);
+                o->h[i] = hf;
+                o->h_lo[i] = lof;
+            }
+        } else {
+            if (!stage) o->h1[i] = h_new;
+            else { hf = 0.5f * (o->h[i] + h_new); o->h[i] = hf; }
+        }
+        if (!stage) { o->hu1[i] = hu_new; o->hv1[i] = hv_new; }
+        else {
+            float huf = 0.5f * (o->hu[i] + hu_new);
+            float hvf = 0.5f * (o->hv[i] + hv_new);
+            if (hf < o->dry_tol) { huf = 0.0f; hvf = 0.0f; }
+            o->hu[i] = huf;
+            o->hv[i] = hvf;
+            if (hf >= o->dry_tol) o->blk[BLK_WORDS * b + BLK_WET] = 1u;
+            if (lam > 1e-30f && A > 1e-10f) {
+                uint32_t v = fbits(o->cfl * A / lam);
+                if (v < o->dt_buf[1]) o->dt_buf[1] = v;
+            }
+        }
+    }
+}
+
+/* Sources as (cell, dh/dt) pairs: all increments first, then the bounds. */
+void oracle_sources(oracle_t *o, const uint32_t *cells, const float *rate, uint32_t count, int compensated) {
+    if (o->dt_buf[0] == 0u) return;
+    float dt = bitsf(o->dt_buf[0]);
+    for (uint32_t k = 0; k < count; ++k) {
+        uint32_t i = cells[k];
+        float inc = dt * rate[k];
+        float h_new;
+        if (compensated) {
+            float lo_new;
+            add_compensated(o->h[i], o->h_lo[i], inc, &h_new, &lo_new);
+            o->h_lo[i] = lo_new;
+        } else {
+            h_new = gmax(o->h[i] + inc, 0.0f);
+        }
+        o->h[i] = h_new;
+        if (h_new >= o->dry_tol) o->blk[BLK_WORDS * (i >> 8) + BLK_WET] = 1u;
+    }
+    for (uint32_t k = 0; k < count; ++k) {
+        uint32_t i = cells[k];
+        float h_new = o->h[i];
+        if (!(h_new >= o->dry_tol)) continue;
+        float u = sqrtf(o->hu[i] * o->hu[i] + o->hv[i] * o->hv[i]) / h_new;
+        float c = sqrtf(o->g * h_new);
+        float lam = 0.0f;
+        for (uint32_t q = o->cptr[i]; q < o->cptr[i + 1u]; ++q) {
+            uint32_t s = o->cidx[q], e = s >> 1;
+            int nb = (s & 1u) ? o->ecL[e] : o->ecR[e];
+            int dry_side = nb >= 0 && o->h[nb] < o->dry_tol;
+            lam += (u + (dry_side ? 2.0f : 1.0f) * c) * o->elen[e];
+        }
+        if (lam > 1e-30f && o->area[i] > 1e-10f) {
+            uint32_t v = fbits(o->cfl * o->area[i] / lam);
+            if (v < o->dt_buf[1]) o->dt_buf[1] = v;
+        }
+    }
+}
+
+void oracle_block_mark(oracle_t *o, int all_active) {
+    for (uint32_t b = 0; b < o->n_blocks; ++b) {
+        if (all_active) { o->blk[BLK_WORDS * b + BLK_WET] = 0u; o->blk[BLK_WORDS * b + BLK_ACTIVE] = 1u; continue; }
+        uint32_t first = b << 8, last = first + 256u < o->N ? first + 256u : o->N, live = 0u;
+        for (uint32_t i = first; i < last; ++i)
+            if (o->h[i] >= o->dry_tol || o->hu[i] != 0.0f || o->hv[i] != 0.0f) { live = 1u; break; }
+        o->blk[BLK_WORDS * b + BLK_WET] = live;
+    }
+}
+
+void oracle_block_dilate(oracle_t *o, int force) {
+    if (!force && o->dt_buf[0] == 0u) return;
+    for (uint32_t b = 0; b < o->n_blocks; ++b) {
+        uint32_t v = o->blk[BLK_WORDS * b + BLK_WET] | o->blk[BLK_WORDS * b + BLK_FORCED];
+        for (uint32_t k = o->bptr[b]; v == 0u && k < o->bptr[b + 1u]; ++k)
+            v = o->blk[BLK_WORDS * o->bidx[k] + BLK_WET] | o->blk[BLK_WORDS * o->bidx[k] + BLK_FORCED];
+        o->blk[BLK_WORDS * b + BLK_ACTIVE] = v;
+    }
+}
+
+void oracle_cfl_prologue(oracle_t *o) {
+    o->dt_buf[0] = fbits(DT_SENTINEL);
+    for (uint32_t eid = 0; eid < o->E; ++eid) {
+        int cL = o->ecL[eid], cR = o->ecR[eid];
+        float nx_ = o->enx[eid], ny_ = o->eny[eid];
+        float hL = o->h[cL], huL = o->hu[cL], hvL = o->hv[cL], hR, huR, hvR;
+        if (cR == -1) {
+            hR = hL;
+            huR = huL - 2.0f * (huL * nx_ + hvL * ny_) * nx_;
+            hvR = hvL - 2.0f * (huL * nx_ + hvL * ny_) * ny_;
+        } else { hR = o->h[cR]; huR = o->hu[cR]; hvR = o->hv[cR]; }
+        float contrib = 0.0f;
+        if (hL >= o->dry_tol || hR >= o->dry_tol)
+            contrib = wave_bound(o, hL, huL, hvL, o->edz[2u * eid], hR, huR, hvR, o->edz[2u * eid + 1u], nx_, ny_) * o->elen[eid];
+        o->ef[EF_WORDS * eid + EF_CFL] = contrib;
+    }
+    for (uint32_t i = 0; i < o->N; ++i) {
+        float lam = 0.0f;
+        for (uint32_t k = o->cptr[i]; k < o->cptr[i + 1u]; ++k) lam += o->ef[EF_WORDS * (o->cidx[k] >> 1) + EF_CFL];
+        if (lam > 1e-30f && o->area[i] > 1e-10f) {
+            uint32_t v = fbits(o->cfl * o->area[i] / lam);
+            if (v < o->dt_buf[0]) o->dt_buf[0] = v;
+        }
+    }
+}
+
+/* mode 0 = START, 1 = STEP, 2 = RETARGET. */
+void oracle_step_control(ctrl_t *c, uint32_t *dt_buf, int mode) {
+    float raw;
+    if (mode == 0) { raw = bitsf(dt_buf[0]); c->last_raw = raw; }
+    else if (mode == 1) {
+        uint32_t done = c->dt_ticks;
+        c->now_ticks += (uint64_t)done;
+        if (done > 0u) { c->steps += 1u; raw = bitsf(dt_buf[1]); c->last_raw = raw; }
+        else raw = c->last_raw;
+    } else raw = c->last_raw;
+    uint64_t remaining = c->stop_ticks > c->now_ticks ? c->stop_ticks - c->now_ticks : 0u;
+    uint32_t ticks;
+    if (remaining == 0u || raw < 1e-10f || raw != raw) ticks = 0u;
+    else if (raw >= 1e10f) ticks = c->dry_dt_ticks;
+    else {
+        float cap = (float)c->dt_max_ticks / TICKS_PER_SECOND;
+        ticks = (uint32_t)(gmin(raw * c->cfl_safety, cap) * TICKS_PER_SECOND);
+    }
+    if (c->dt_max_ticks < ticks) ticks = c->dt_max_ticks;
+    if ((uint64_t)ticks > remaining) ticks = (uint32_t)remaining;
+    c->dt_ticks = ticks;
+    dt_buf[0] = fbits((float)ticks / TICKS_PER_SECOND);
+    dt_buf[1] = fbits(DT_SENTINEL);
+}
+
+/* One whole resident step as the reference records it (gpu_resident_batch.py:489-513). */
+void oracle_step(oracle_t *o, const uint32_t *src_cells, const float *src_rate, uint32_t n_src, int compensated,
+                 int track_clamp, int active_set) {
+    for (int stage = 0; stage < 2; ++stage) {
+        oracle_flux_stage(o, stage);
+        oracle_update_stage(o, stage, compensated, track_clamp);
+    }
+    if (n_src) oracle_sources(o, src_cells, src_rate, n_src, compensated);
+    if (active_set) oracle_block_dilate(o, 0);
+    oracle_step_control(o->ctrl, o->dt_buf, 1);
+}
+
+float oracle_pow43(float x) { return pow43(x); }
+
+void oracle_hllc(float g, float dry_tol, const float *in6, float *out4) {
+    oracle_t o;
+    memset(&o, 0, sizeof o);
+    o.g = g;
+    o.dry_tol = dry_tol;
+    hllc(&o, in6[0], in6[1], in6[2], in6[3], in6[4], in6[5], &out4[0], &out4[1], &out4[2], &out4[3]);
+}
+
+void oracle_hllc_speeds(float g, float dry_tol, const float *in4, float *out2) {
+    oracle_t o;
+    memset(&o, 0, sizeof o);
+    o.g = g;
+    o.dry_tol = dry_tol;
+    hllc_speeds(&o, in4[0], in4[1], in4[2], in4[3], &out2[0], &out2[1]);
+}
+
+void oracle_two_sum(float a, float b, float *se) { two_sum(a, b, &se[0], &se[1]); }
+
+size_t oracle_sizeof(void) { return sizeof(oracle_t); }
+size_t oracle_ctrl_sizeof(void) { return sizeof(ctrl_t); }
