@@ -1,0 +1,526 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 shallow-water step (one JSON line on rank 0).
+
+Workload (default): the 1M-cell forward run -- a seeded Voronoi mesh over a
+10 km square on fractal terrain (beta 2, 20 m relief, 3 m channel), a 4 m
+circular dam of 500 m radius, n = 0.035, float32 state, CFL 0.8 per step.
+A step is one Heun step of the whole mesh (blocks outside the two-ring of
+wet blocks are skipped, as in the reference's resident backend).
+
+* ``value``: cells x steps / device time of exactly ``--steps`` steps after
+  ``--warmup`` steps, inputs resident in HBM, steps replayed as CUDA graphs.
+* ``computed_cell_steps_per_s``: the same over the cells actually computed.
+* ``roofline``: the fused stage kernel's algorithmic bytes over its mean
+  launch time (CUDA events recorded inside the graphs), against the measured
+  HBM copy bandwidth.
+* ``e2e``: the same metric through the public ``run()`` call with host
+  arrays: upload of the initial state, the run, control-block reads after
+  every submit, download of the final state.
+* ``cpu_baseline``: the float64 oracle step timed on one host core on the
+  same mesh; its result also gives the stated float64 error of the CUDA step.
+
+``--impl reference`` times the reference's CPU step (its float64 NumPy
+restatement) on all host cores instead; under torchrun only rank 0 works.
+With N GPUs every rank runs an independent replica (the single-mesh path
+does not shard): ``value`` is the sum of the replicas' cell-steps over the
+slowest rank's time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "cell-steps/s fwd and fwd+adjoint, plain vs batched, at stated FP64-oracle error"
+UNIT = "cell-steps/s"
+L2_BYTES = 126 * 2**20
+SENTINEL_STOP = 1 << 62
+
+
+def parse_args() -> argparse.Namespace:
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", choices=["dam_break", "full_wet"], default="dam_break")
+    ap.add_argument("--cells", type=int, default=1_000_000)
+    ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--chunk", type=int, default=500, help="steps per captured graph in the timed region")
+    return ap.parse_args()
+
+
+# -- workload ----------------------------------------------------------------------------------
+def build_scenario(name: str, cells: int, seed: int):
+    from inundation_b200 import scenarios
+
+    side = 10_000.0 * np.sqrt(cells / 1_000_000)
+    sc = scenarios.dam_break(cells, seed=seed, side=side)
+    if name == "full_wet":
+        # Every block active for the whole run: still water 1 m over the highest bed plus a current.
+        zb = sc.geom.zb.astype(np.float64)
+        h = (float(zb.max()) + 1.0 - zb).astype(np.float32)
+        x = sc.geom.world_centroid[:, 0]
+        sc.h0 = h
+        sc.hu0 = (0.2 * np.sin(2 * np.pi * x / side) * h).astype(np.float32)
+        sc.name = "full_wet"
+    return sc
+
+
+def workload_config(sc, args) -> dict:
+    g = sc.geom
+    from inundation_b200.layout import algorithmic_bytes_per_cell_step
+
+    per_step = algorithmic_bytes_per_cell_step(g) * g.N
+    return {
+        "workload": f"{sc.name}_{g.N // 1000}k_voronoi",
+        "cells": int(g.N),
+        "edges": int(g.E),
+        "csr_slots": int(g.cell_edge_ptr[-1]),
+        "max_degree": int(g.max_degree),
+        "terrain": "fractal beta 2, 20 m relief, 3 m channel",
+        "dam": "4 m depth within 500 m of the centre" if sc.name == "dam_break" else "still water + current, all wet",
+        "manning_n": 0.035,
+        "cfl": 0.8,
+        "active_set": True,
+        "compensated": True,
+        "seed": args.seed,
+        "l2": f"inputs larger than L2: {per_step / 2**20:.0f} MiB algorithmic traffic per full step, "
+        f"{L2_BYTES // 2**20} MiB L2; no flush",
+        "parallelism": f"replicas{args.gpus}" if args.gpus > 1 else "single",
+    }
+
+
+# -- clocks ------------------------------------------------------------------------------------
+class ClockSampler:
+    """``nvidia-smi`` clock and throttle samples every 200 ms while running."""
+
+    QUERY = (
+        "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+        "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+        "clocks_event_reasons.sw_power_cap"
+    )
+
+    def __init__(self, index: int) -> None:
+        self.index = index
+        self.proc: subprocess.Popen | None = None
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self) -> None:
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"],
+                stdout=self.file, stderr=subprocess.DEVNULL,
+            )
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        self.file.flush()
+        rows = [r.split(", ") for r in Path(self.file.name).read_text().strip().splitlines() if r.count(",") >= 8]
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip() == "Active"})
+        load = sorted(sm)[len(sm) // 2:] if sm else []
+        return {
+            "sm_mhz": float(np.median(load)) if load else None,
+            "sm_max_mhz": max(mx) if mx else None,
+            "reasons": reasons,
+            "samples": len(rows),
+        }
+
+
+# -- distributed plumbing ---------------------------------------------------------------------
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def reduce_max(value: float, world: int) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int) -> None:
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def peaks() -> tuple[float, str]:
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        return float(json.loads(path.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# -- CUDA arm ------------------------------------------------------------------------------------
+def plan(solver, sc) -> None:
+    from inundation_b200.tuning import dt_to_ticks
+
+    c = solver._ctrl
+    c[...] = 0
+    c["stop_ticks"] = SENTINEL_STOP
+    c["dt_max_ticks"] = dt_to_ticks(sc.dt_max)
+    c["dry_dt_ticks"] = dt_to_ticks(min(sc.dt_init, sc.dt_max))
+    c["cfl_safety"] = solver.cfl_safety
+    solver._sync_ctrl_to_device()
+    solver._enqueue_prologue()
+    solver._read_ctrl()
+
+
+def capture_chunks(solver, steps: int, chunk: int, timed: bool):
+    """Graphs covering exactly ``steps`` steps; with ``timed``, events around every stage launch."""
+    import ctypes
+
+    import torch
+
+    from inundation_b200 import native
+
+    graphs, events = [], []
+    params, sources = solver._params(), solver._sources()
+    mesh, state = ctypes.byref(solver._mesh), ctypes.byref(solver._state)
+    left = steps
+    while left > 0:
+        n = min(chunk, left)
+        left -= n
+        g = torch.cuda.CUDAGraph()
+        ev = [torch.cuda.Event(enable_timing=True, external=True) for _ in range(3 * n + 1)] if timed else []
+        solver._stream.synchronize()
+        with torch.cuda.graph(g, stream=solver._stream):
+            st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+            for k in range(n):
+                if timed:
+                    ev[3 * k].record()
+                native.check(solver._lib.swe_stage(mesh, state, ctypes.byref(params), 0, st), "stage 0")
+                if timed:
+                    ev[3 * k + 1].record()
+                native.check(solver._lib.swe_stage(mesh, state, ctypes.byref(params), 1, st), "stage 1")
+                if timed:
+                    ev[3 * k + 2].record()
+                if sources.count:
+                    native.check(solver._lib.swe_apply_sources(mesh, state, ctypes.byref(params), ctypes.byref(sources), st), "sources")
+                native.check(solver._lib.swe_block_dilate_compact(mesh, state, ctypes.byref(params), 0, 1, st), "dilate")
+            if timed:
+                ev[3 * n].record()
+        graphs.append(g)
+        events.append(ev)
+    return graphs, events
+
+
+def cpu_baseline_and_error(sc, solver_cls, device: str) -> tuple[dict, dict]:
+    """FP64 oracle steps on one core (timed) and the CUDA step's error against them."""
+    import torch
+
+    from oracle import fp64_step
+
+    g = sc.geom
+    s0 = fp64_step.State(*(a.astype(np.float64) for a in (sc.h0, sc.hu0, sc.hv0)))
+    dt_cfl = fp64_step.cfl_dt(g, s0, g=9.81, dry_tol=sc.dry_tol, cfl=0.8)
+    dt = 2.0 ** np.floor(np.log2(min(dt_cfl, 1.0)))
+    steps = 3
+    n64 = sc.manning.astype(np.float64)
+    fp64_step.heun_step(g, s0, n64, dt, g=9.81, dry_tol=sc.dry_tol)  # warm caches
+    t0 = time.perf_counter()
+    s = s0
+    for _ in range(steps):
+        s = fp64_step.heun_step(g, s, n64, dt, g=9.81, dry_tol=sc.dry_tol)
+    wall = time.perf_counter() - t0
+    solver = solver_cls(g, None, sc.h0, sc.hu0, sc.hv0, sc.manning, dry_tol=sc.dry_tol, device=device)
+    solver.run(t_end=steps * dt, output_interval_s=steps * dt, dt_max=dt, dt_init=dt, cfl_interval=1, progress=False)
+    h, hu, hv = solver.download_h_precise(), solver.download_hu(), solver.download_hv()
+    del solver
+    torch.cuda.empty_cache()
+    cpu = {
+        "value": g.N * steps / wall,
+        "unit": UNIT,
+        "cores": 1,
+        "kind": "port",
+        "sample": f"{steps} float64 Heun steps (dt={dt:g} s) of the full {g.N}-cell mesh, single process",
+    }
+    err = {
+        "steps": steps,
+        "dt_s": dt,
+        "h_max_abs_m": float(np.abs(h - s.h).max()),
+        "hu_max_abs": float(np.abs(hu - s.hu).max()),
+        "hv_max_abs": float(np.abs(hv - s.hv).max()),
+        "tolerance_h_m": 1e-5,
+    }
+    return cpu, err
+
+
+def run_b200(args, world: int, rank: int, local: int) -> None:
+    import torch
+
+    from inundation_b200.backend import SWESolverB200Resident
+    from inundation_b200.layout import algorithmic_bytes_per_cell_step
+
+    device = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    sc = build_scenario(args.workload, args.cells, args.seed)
+    g = sc.geom
+    solver = SWESolverB200Resident(g, None, sc.h0, sc.hu0, sc.hv0, sc.manning, dry_tol=sc.dry_tol, device=device)
+    plan(solver, sc)
+    warm, _ = capture_chunks(solver, args.warmup, args.chunk, timed=False)
+    graphs, events = capture_chunks(solver, args.steps, args.chunk, timed=True)
+    for gr in warm:
+        gr.replay()
+    solver._stream.synchronize()
+    computed0 = solver.computed_cells
+    solver._read_ctrl()
+    steps0, t0_ticks = int(solver._ctrl["steps"][0]), int(solver._ctrl["now_ticks"][0])
+
+    clocks = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(solver._stream):
+        start.record()
+        for gr in graphs:
+            gr.replay()
+        end.record()
+    torch.cuda.synchronize()
+    clock = clocks.stop()
+    barrier(world)
+    ms = start.elapsed_time(end)
+    ms_max = reduce_max(ms, world)
+
+    solver._read_ctrl()
+    done = int(solver._ctrl["steps"][0]) - steps0
+    if done != args.steps:
+        raise RuntimeError(f"timed region ran {done} real steps, expected {args.steps} (the clock stalled)")
+    t_sim = (int(solver._ctrl["now_ticks"][0]) - t0_ticks) / 2**20
+    computed = solver.computed_cells - computed0
+    stage_ms = 0.0
+    dilate_ms = 0.0
+    for ev in events:
+        n = (len(ev) - 1) // 3
+        for k in range(n):
+            stage_ms += ev[3 * k].elapsed_time(ev[3 * k + 1]) + ev[3 * k + 1].elapsed_time(ev[3 * k + 2])
+            dilate_ms += ev[3 * k + 2].elapsed_time(ev[3 * k + 3])
+    launches = 2 * args.steps
+    bpc = algorithmic_bytes_per_cell_step(g)
+    alg_bytes = computed * bpc  # over all stage launches of the timed region
+    achieved = alg_bytes / (stage_ms * 1e-3) / 1e9
+    peak, peak_kind = peaks()
+    traffic = None
+    tfile = ROOT / "profiles" / "stage_kernel_traffic.json"
+    if tfile.exists():
+        per_cell = json.loads(tfile.read_text()).get("dram_bytes_per_computed_cell_step")
+        if per_cell:
+            traffic = per_cell * computed / launches
+    value = world * g.N * args.steps / (ms_max * 1e-3)
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic: seeded Voronoi mesh, fractal DEM (no real DEM or mesh files)",
+        "config": workload_config(sc, args),
+        "mode": "forward, plain (one mesh per GPU)",
+        "computed_cell_steps_per_s": world * computed / (ms_max * 1e-3),
+        "active_fraction": computed / (g.N * args.steps),
+        "simulated_s": t_sim,
+        "gpu_launches": 3 * args.steps,
+        "roofline": {
+            "bound": "hbm",
+            "achieved": achieved,
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": achieved / peak,
+            "traffic": traffic,
+            "kernel": "stage_kernel (fused edge flux + gather + Heun update), both stages",
+            "algorithmic_bytes_per_cell_step": bpc,
+            "launches": launches,
+            "mean_launch_us": stage_ms * 1e3 / launches,
+            "peak_kind": f"{peak_kind} HBM copy bandwidth",
+            "stage_share_of_step": stage_ms / (stage_ms + dilate_ms),
+        },
+        "clocks": clock,
+    }
+    if rank == 0 and not args.no_e2e:
+        line["e2e"] = e2e_run(solver, sc, t_sim, args)
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        del graphs, warm
+        cpu, err = cpu_baseline_and_error(sc, SWESolverB200Resident, device)
+        line["cpu_baseline"] = cpu
+        line["fp64_oracle_error"] = err
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def e2e_run(solver, sc, t_sim: float, args) -> dict:
+    """The public reset() + run() + download_*() calls with host arrays, timed on the host clock."""
+    from inundation_b200.tuning import seconds_to_ticks
+
+    t_end = max(seconds_to_ticks(t_sim) / 2**20, 1.0 / 2**20)
+    solver.run(t_end=min(t_end, 1.0), output_interval_s=t_end, dt_max=sc.dt_max, dt_init=sc.dt_init, cfl_interval=1,
+               progress=False)  # capture the submit graph outside the timed region
+    before = solver.steps_total
+    t0 = time.perf_counter()
+    solver.reset(sc.h0, sc.hu0, sc.hv0)
+    solver.run(t_end=t_end, output_interval_s=t_end, dt_max=sc.dt_max, dt_init=sc.dt_init, cfl_interval=1,
+               progress=False, resume=True, t_start=0.0)
+    solver.download_h(), solver.download_hu(), solver.download_hv()
+    wall = time.perf_counter() - t0
+    steps = solver.steps_total - before
+    submits = -(-steps // solver.steps_per_graph)
+    n = sc.geom.N
+    # H2D: h, hu, hv and one control block; D2H: the run's initial, window-end and final depth,
+    # the three final arrays, and a control block after the prologue and after every submit.
+    return {
+        "value": n * steps / wall,
+        "unit": UNIT,
+        "steps": steps,
+        "wall_s": wall,
+        "h2d_bytes_per_step": (12 * n + 48) / steps,
+        "d2h_bytes_per_step": (24 * n + 48 * (submits + 1)) / steps,
+        "path": "SWESolverB200Resident.reset(host h, hu, hv) + run(t_end) + download_h/hu/hv",
+    }
+
+
+# -- reference arm ---------------------------------------------------------------------------------
+_WORKER: dict = {}
+
+
+def _ref_worker_init(cells: int, seed: int) -> None:
+    os.environ["OMP_NUM_THREADS"] = "1"
+    sys.path.insert(0, str(ROOT))
+    from inundation_b200 import scenarios
+    from oracle import fp64_step
+
+    side = 10_000.0 * np.sqrt(cells / 1_000_000)
+    sc = scenarios.dam_break(cells, seed=seed, side=side)
+    s = fp64_step.State(*(a.astype(np.float64) for a in (sc.h0, sc.hu0, sc.hv0)))
+    dt = min(fp64_step.cfl_dt(sc.geom, s, g=9.81, dry_tol=sc.dry_tol, cfl=0.8), 1.0)
+    _WORKER.update(geom=sc.geom, state=s, n=sc.manning.astype(np.float64), dt=dt, dry=sc.dry_tol)
+
+
+def _ref_worker_step(_: int) -> int:
+    from oracle import fp64_step
+
+    w = _WORKER
+    w["state"] = fp64_step.heun_step(w["geom"], w["state"], w["n"], w["dt"], g=9.81, dry_tol=w["dry"])
+    return int(w["geom"].N)
+
+
+def run_reference(args, world: int, rank: int) -> None:
+    if rank != 0:
+        return
+    import multiprocessing as mp
+
+    procs = max(1, min(os.cpu_count() or 1, 64))
+    budget_s = 150.0
+    per_core_rate = 3.0e5
+    cells = int(np.clip(budget_s * per_core_rate / (args.steps + args.warmup), 2000, args.cells))
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs, initializer=_ref_worker_init, initargs=(cells, args.seed)) as pool:
+        for _ in range(args.warmup):
+            pool.map(_ref_worker_step, range(procs), chunksize=1)
+        t0 = time.perf_counter()
+        total = 0
+        for _ in range(args.steps):
+            total += sum(pool.map(_ref_worker_step, range(procs), chunksize=1))
+        wall = time.perf_counter() - t0
+    value = total / wall
+    sc_cfg = {
+        "workload": f"dam_break_{args.cells // 1000}k_voronoi",
+        "cells": args.cells,
+        "sample_cells_per_process": cells,
+        "parallelism": f"{procs} processes",
+        "seed": args.seed,
+    }
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": wall * 1e3 / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic: seeded Voronoi mesh, fractal DEM",
+        "config": sc_cfg,
+        "cpu_baseline": {
+            "value": value,
+            "unit": UNIT,
+            "cores": procs,
+            "kind": "port",
+            "sample": f"each step: one float64 Heun step of a {cells}-cell sample of the workload (same cell "
+            f"size, terrain and dam) in each of {procs} processes",
+        },
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    args = parse_args()
+    if args.impl == "reference":
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        run_reference(args, world, rank)
+        return
+    world, rank, local = dist_setup()
+    try:
+        run_b200(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

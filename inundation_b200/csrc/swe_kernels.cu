@@ -290,41 +290,54 @@ __global__ void step_control_kernel(swe_ctrl_t *c, uint32_t *dt_buf, int mode) {
 // ---------------------------------------------------------------------------
 // Dilation of the wet marks over each block's two-ring, compaction of the
 // active blocks, then (last CTA) step control (resident.py:778-805, 813-885).
+// One warp per block reads the block's two-ring in parallel; each CTA of
+// kDilateWarps warps appends its active blocks with one atomic, in order.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads)
+constexpr int kDilateWarps = 32;
+
+__global__ void __launch_bounds__(kDilateWarps * 32)
     dilate_compact_kernel(swe_mesh_t m, swe_state_t s, int all_active, int force, int control_mode) {
     const bool run = force || s.dt_buf[0] != 0u;
-    const uint32_t b = blockIdx.x * kThreads + threadIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t b = blockIdx.x * kDilateWarps + warp;
+    __shared__ uint32_t flag[kDilateWarps];
+    __shared__ bool last;
     if (run) {
         uint32_t v = 0u;
         if (b < m.n_blocks) {
             if (all_active) {
                 v = 1u;
             } else {
-                v = s.blk[kBlkWords * b + kBlkWet] | s.blk[kBlkWords * b + kBlkForced];
-                for (uint32_t k = m.ring_ptr[b]; v == 0u && k < m.ring_ptr[b + 1]; ++k) {
+                const uint32_t k0 = m.ring_ptr[b], k1 = m.ring_ptr[b + 1];
+                if (lane == 0) v = s.blk[kBlkWords * b + kBlkWet] | s.blk[kBlkWords * b + kBlkForced];
+                for (uint32_t k = k0 + lane; k < k1; k += 32) {
                     const uint32_t nb = m.ring_idx[k];
-                    v = s.blk[kBlkWords * nb + kBlkWet] | s.blk[kBlkWords * nb + kBlkForced];
+                    v |= s.blk[kBlkWords * nb + kBlkWet] | s.blk[kBlkWords * nb + kBlkForced];
                 }
+                v = __any_sync(0xFFFFFFFFu, v != 0u) ? 1u : 0u;
             }
-            s.blk[kBlkWords * b + kBlkActive] = v;
+            if (lane == 0) s.blk[kBlkWords * b + kBlkActive] = v;
         }
-        const unsigned ballot = __ballot_sync(0xFFFFFFFFu, v != 0u);
-        const int lane = threadIdx.x & 31;
-        const uint32_t cells = (v != 0u) ? min(static_cast<uint32_t>(kBlockCells), m.n_cells - b * kBlockCells) : 0u;
-        const uint32_t warp_cells = __reduce_add_sync(0xFFFFFFFFu, cells);
-        uint32_t pos = 0;
-        if (lane == 0 && ballot) {
-            pos = atomicAdd(&s.sched[kSchedNext], static_cast<uint32_t>(__popc(ballot)));
-            atomicAdd(&s.sched[kSchedNextCells], warp_cells);
+        if (lane == 0) flag[warp] = v;
+        __syncthreads();
+        if (warp == 0) {
+            const uint32_t blk = blockIdx.x * kDilateWarps + lane;
+            const bool on = flag[lane] != 0u;
+            const unsigned ballot = __ballot_sync(0xFFFFFFFFu, on);
+            const uint32_t cells = on ? min(static_cast<uint32_t>(kBlockCells), m.n_cells - blk * kBlockCells) : 0u;
+            const uint32_t total_cells = __reduce_add_sync(0xFFFFFFFFu, cells);
+            uint32_t pos = 0;
+            if (lane == 0 && ballot) {
+                pos = atomicAdd(&s.sched[kSchedNext], static_cast<uint32_t>(__popc(ballot)));
+                atomicAdd(&s.sched[kSchedNextCells], total_cells);
+            }
+            pos = __shfl_sync(0xFFFFFFFFu, pos, 0);
+            const uint32_t slot = pos + __popc(ballot & ((1u << lane) - 1u));
+            if (on && slot < m.n_blocks) s.active_list[slot] = blk;
         }
-        pos = __shfl_sync(0xFFFFFFFFu, pos, 0);
-        const uint32_t slot = pos + __popc(ballot & ((1u << lane) - 1u));
-        if (v != 0u && slot < m.n_blocks) s.active_list[slot] = b;
     }
     __threadfence();
     __syncthreads();
-    __shared__ bool last;
     if (threadIdx.x == 0) last = atomicAdd(&s.sched[kSchedDone], 1u) == gridDim.x - 1;
     __syncthreads();
     if (!last || threadIdx.x != 0) return;
@@ -597,8 +610,8 @@ int swe_apply_sources(const swe_mesh_t *mesh, const swe_state_t *state, const sw
 int swe_block_dilate_compact(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params_t *params, int force,
                              int control_mode, swe_stream_t stream) {
     if (!mesh_ok(mesh) || !state_ok(state) || !params || control_mode < -1 || control_mode > 2) return SWE_ERR_ARGUMENT;
-    const uint32_t grid = (mesh->n_blocks + kThreads - 1) / kThreads;
-    dilate_compact_kernel<<<grid, kThreads, 0, stream>>>(*mesh, *state, params->active_set ? 0 : 1, force, control_mode);
+    const uint32_t grid = (mesh->n_blocks + kDilateWarps - 1) / kDilateWarps;
+    dilate_compact_kernel<<<grid, kDilateWarps * 32, 0, stream>>>(*mesh, *state, params->active_set ? 0 : 1, force, control_mode);
     return check_launch();
 }
 

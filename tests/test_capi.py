@@ -1,0 +1,96 @@
+"""The C ABI library loads and exports every function ``include/*.h`` declares (no GPU needed).
+
+Also the host-side layout the kernels index: every CSR slot of a cell must
+name, through its tile position, the edge the reference's remapped CSR names
+(``inundation/mesh/blocks.py:33-44``), with the cell on the stated side, and
+the kernels' launch arguments must refuse null pointers.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from inundation_b200 import native
+from inundation_b200.build import LIB_PATH, build
+from inundation_b200.layout import TILE_ALIGN, build_tile_layout
+from inundation_b200.mesh.blocks import edge_order_by_block, remap_cell_edges
+from inundation_b200.mesh.geometry import build_geometry, hilbert_reorder
+
+HEADERS = sorted((Path(__file__).resolve().parent.parent / "include").glob("*.h"))
+GEO = np.load(Path(__file__).parent / "golden" / "geometry.npz")
+
+
+def declared_functions() -> list[str]:
+    names: list[str] = []
+    for header in HEADERS:
+        text = re.sub(r"/\*.*?\*/", "", header.read_text(), flags=re.S)
+        names += re.findall(r"^\s*(?:const\s+)?[a-z_0-9]+\s*\*?\s*(swe_[a-z0-9_]+)\s*\(", text, flags=re.M)
+    return sorted(set(names))
+
+
+@pytest.fixture(scope="module")
+def lib() -> ctypes.CDLL:
+    build()
+    return native.load()
+
+
+def test_library_is_built_in_tree() -> None:
+    build()
+    assert LIB_PATH.exists() and LIB_PATH.is_relative_to(Path(native.__file__).resolve().parent)
+
+
+def test_every_declared_function_is_exported(lib: ctypes.CDLL) -> None:
+    names = declared_functions()
+    assert len(names) >= 15
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, f"declared but not exported: {missing}"
+    assert set(names) == set(native.exported_symbols())
+
+
+def test_status_strings_and_argument_checks(lib: ctypes.CDLL) -> None:
+    assert lib.swe_status_string(0) == b"ok"
+    assert b"argument" in lib.swe_status_string(1)
+    # Null structs are refused before anything touches a device.
+    assert lib.swe_stage(None, None, None, 0, None) == 1
+    assert lib.swe_step(None, None, None, None, None) == 1
+    assert lib.swe_prologue(None, None, None, None) == 1
+    assert lib.swe_step_control(None, None, 0, None) == 1
+    assert lib.swe_volume_fp64(None, None, None, 0, None, None, None) == 1
+    assert lib.swe_workspace_bytes(1_000_000) > 3907 * 4
+    assert lib.swe_tile_smem_bytes(900) >= 900 * 24
+
+
+def test_ctypes_structs_match_the_header_layout() -> None:
+    assert ctypes.sizeof(native.SweMesh) == 16 + 15 * 8
+    assert ctypes.sizeof(native.SweState) == 14 * 8
+    assert ctypes.sizeof(native.SweParams) == 32
+    assert ctypes.sizeof(native.SweSources) == 24
+
+
+@pytest.mark.parametrize("name", ["voronoi", "valley", "mixed"])
+def test_tile_layout_resolves_every_csr_slot(name: str) -> None:
+    offsets = GEO[f"{name}_in_offsets"]
+    raw = build_geometry(GEO[f"{name}_in_verts"], GEO[f"{name}_in_faces"], offsets if offsets.size else None,
+                         zb_from_file=GEO[f"{name}_in_zb"])
+    g = hilbert_reorder(raw, verbose=False)[0]
+    L = build_tile_layout(g)
+    order = edge_order_by_block(g.edge_cellL, 256)
+    signed = remap_cell_edges(g.cell_edge_idx_signed, order).astype(np.int64)
+    cell = np.repeat(np.arange(g.N), np.diff(g.cell_edge_ptr))
+    blk = cell // 256
+    local, side = L.lcsr.astype(np.int64) >> 1, L.lcsr.astype(np.int64) & 1
+    rec = L.tile_ptr[blk].astype(np.int64) + local
+    assert (local < L.tile_count[blk]).all()
+    np.testing.assert_array_equal(L.tile_edge[rec], signed >> 1)
+    np.testing.assert_array_equal(side, signed & 1)
+    np.testing.assert_array_equal(np.where(side == 1, L.tile_cr[rec], L.tile_cl[rec]), cell)
+    assert (L.tile_ptr % TILE_ALIGN == 0).all()
+    # every edge is in the tile of its left cell's block exactly once
+    owned = L.tile_edge[L.tile_edge >= 0]
+    assert np.bincount(owned, minlength=g.E).min() >= 1
+    assert L.max_tile_edges == int(L.tile_count.max())
