@@ -27,7 +27,8 @@ enum swe_status {
     SWE_OK = 0,
     SWE_ERR_ARGUMENT = 1,     /* a null pointer, a zero size or an unknown mode */
     SWE_ERR_CUDA = 2,         /* a CUDA launch or runtime call failed */
-    SWE_ERR_TOO_LARGE = 3,    /* a block's edge tile does not fit in shared memory */
+    SWE_ERR_TOO_LARGE = 3,    /* a size beyond a fixed limit: a block's edge tile larger than shared
+                                 memory, or more cells than swe_volume_fp64_noalloc's static scratch holds */
     SWE_ERR_MATH = 4,         /* the device arithmetic lost the two-sum error term */
 };
 
@@ -167,6 +168,19 @@ int swe_step(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params_
 uint32_t swe_volume_partials(uint32_t n_cells);
 int swe_volume_fp64(const float *h, const float *h_lo, const float *area, uint32_t n_cells, double *partials,
                     double *out, swe_stream_t stream);
+
+/* swe_volume_fp64 for callers that cannot allocate device memory (a host
+   under a fixed device-memory budget, an application that owns the CUDA
+   allocator, code running where cudaMalloc is not allowed). No counterpart in
+   the reference, which sums the volume on the host. The partial sums live in
+   a static 8 KiB device array that every GPU loading this library holds until
+   exit, so n_cells is limited to 4,194,304 (SWE_ERR_TOO_LARGE above). Call it
+   with the stream's device current; its first call on a device looks up the
+   array's address, so make that first call before any stream capture. All
+   calls share the array: calls that overlap on the GPU (other streams, other
+   threads) race and must be serialised by the caller. */
+int swe_volume_fp64_noalloc(const float *h, const float *h_lo, const float *area, uint32_t n_cells, double *out,
+                            swe_stream_t stream);
 
 /* The two-sum of (v[0], v[1]) into v[2] (its error term) on the device: the
    reference's fast-math guard (inundation/vulkan/solver.py:449-467,

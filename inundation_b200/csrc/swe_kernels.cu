@@ -13,6 +13,7 @@
 // the lines each kernel replaces.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 
 #include "../../include/inundation_b200.h"
@@ -698,10 +699,65 @@ const char *swe_status_string(int status) {
         case SWE_OK: return "ok";
         case SWE_ERR_ARGUMENT: return "invalid argument";
         case SWE_ERR_CUDA: return "CUDA launch or runtime error";
-        case SWE_ERR_TOO_LARGE: return "a block's edge tile does not fit in shared memory";
+        case SWE_ERR_TOO_LARGE:
+            return "size beyond a fixed limit (an edge tile larger than shared memory, or more cells than the "
+                   "allocation-free volume's static scratch holds)";
         case SWE_ERR_MATH: return "device arithmetic lost the two-sum error term";
         default: return "unknown status";
     }
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free float64 volume.
+//
+// For callers that must not allocate device memory during a run: a host that
+// runs under a fixed device-memory budget checked at start-up, an embedding
+// application that owns the CUDA allocator, or code called from a context
+// where cudaMalloc is not allowed. The per-CTA partial sums that
+// swe_volume_fp64 takes from its caller live here in a static device array
+// instead; every GPU that loads this library holds it (8 KiB) until exit.
+// ---------------------------------------------------------------------------
+namespace swe {
+
+constexpr uint32_t kNoAllocPartials = 1024;
+constexpr uint32_t kNoAllocCellsPerPartial = 4096;
+constexpr uint32_t kNoAllocMaxCells = kNoAllocPartials * kNoAllocCellsPerPartial;
+constexpr int kNoAllocDevices = 64;
+
+static __device__ __align__(256) double g_volume_scratch[kNoAllocPartials];
+
+// Device address of g_volume_scratch per device ordinal. In host code the
+// array's name is only a host-side stand-in, never a device address.
+static std::atomic<double *> g_volume_scratch_addr[kNoAllocDevices];
+
+}  // namespace swe
+
+extern "C" int swe_volume_fp64_noalloc(const float *h, const float *h_lo, const float *area, uint32_t n_cells,
+                                       double *out, swe_stream_t stream) {
+    if (!h || !area || !out || n_cells == 0u) return SWE_ERR_ARGUMENT;
+    if (n_cells > kNoAllocMaxCells) return SWE_ERR_TOO_LARGE;
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return SWE_ERR_CUDA;
+    if (dev < 0 || dev >= kNoAllocDevices) return SWE_ERR_ARGUMENT;
+    double *scratch = g_volume_scratch_addr[dev].load(std::memory_order_acquire);
+    if (scratch == nullptr) {
+        // First call on this device (the device must be current): look up the
+        // array's device address once and keep it.
+        void *addr = nullptr;
+        if (cudaGetSymbolAddress(&addr, g_volume_scratch) != cudaSuccess || addr == nullptr) return SWE_ERR_CUDA;
+        scratch = static_cast<double *>(addr);
+        g_volume_scratch_addr[dev].store(scratch, std::memory_order_release);
+    }
+    // Same partition as swe_volume_fp64 (one partial per 4096 cells below the
+    // limit), so both entry points sum in the same order. Every partial the
+    // final pass reads is rewritten first, so the array needs no clearing.
+    const uint32_t parts = swe_volume_partials(n_cells);
+    const uint32_t per = (n_cells + parts - 1) / parts;
+    volume_partial_kernel<<<parts, kThreads, 0, stream>>>(h, h_lo, area, n_cells, per, scratch);
+    int rc = check_launch();
+    if (rc) return rc;
+    volume_final_kernel<<<1, kThreads, 0, stream>>>(scratch, parts, out);
+    return check_launch();
+}

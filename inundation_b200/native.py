@@ -17,7 +17,8 @@ _U32 = ctypes.c_uint32
 STATUS_MESSAGES = {
     1: "invalid argument",
     2: "CUDA launch or runtime error",
-    3: "a block's edge tile does not fit in shared memory",
+    3: "size beyond a fixed limit (an edge tile larger than shared memory, or more cells than the "
+    "allocation-free volume's static scratch holds)",
     4: "device arithmetic lost the two-sum error term",
 }
 
@@ -36,6 +37,7 @@ _SIGNATURES: dict[str, tuple[list, object]] = {
     "swe_step": ([_P, _P, _P, _P, _P], ctypes.c_int),
     "swe_volume_partials": ([_U32], _U32),
     "swe_volume_fp64": ([_P, _P, _P, _U32, _P, _P, _P], ctypes.c_int),
+    "swe_volume_fp64_noalloc": ([_P, _P, _P, _U32, _P, _P], ctypes.c_int),
     "swe_eft_probe": ([_P, _P], ctypes.c_int),
     "swe_pow43": ([_P, _P, _U32, _P], ctypes.c_int),
     "swe_status_string": ([ctypes.c_int], ctypes.c_char_p),
