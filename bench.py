@@ -60,6 +60,7 @@ def parse_args() -> argparse.Namespace:
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--chunk", type=int, default=500, help="steps per captured graph in the timed region")
+    ap.add_argument("--kernel", choices=["staged", "plain"], default="staged", help="stage kernel variant")
     return ap.parse_args()
 
 
@@ -298,6 +299,7 @@ def run_b200(args, world: int, rank: int, local: int) -> None:
     sc = build_scenario(args.workload, args.cells, args.seed)
     g = sc.geom
     solver = SWESolverB200Resident(g, None, sc.h0, sc.hu0, sc.hv0, sc.manning, dry_tol=sc.dry_tol, device=device)
+    solver.stage_kernel = args.kernel
     plan(solver, sc)
     warm, _ = capture_chunks(solver, args.warmup, args.chunk, timed=False)
     graphs, events = capture_chunks(solver, args.steps, args.chunk, timed=True)
@@ -376,7 +378,7 @@ def run_b200(args, world: int, rank: int, local: int) -> None:
             "unit": "GB/s",
             "frac": achieved / peak,
             "traffic": traffic,
-            "kernel": "stage_kernel (fused edge flux + gather + Heun update), both stages",
+            "kernel": f"stage kernel, {args.kernel} (fused edge flux + gather + Heun update), both stages",
             "algorithmic_bytes_per_cell_step": bpc,
             "launches": launches,
             "mean_launch_us": stage_ms * 1e3 / launches,

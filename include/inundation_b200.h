@@ -43,22 +43,27 @@ typedef struct {
     uint32_t dry_dt_ticks;
     float last_raw;
     float cfl_safety;
-    uint32_t pad;
+    uint32_t error;  /* set by the device: 1 = a bounded wait for staged data timed out */
 } swe_ctrl_t;
 
 /* Static mesh in the block-tile layout (device pointers).
    Block b = cells [256 b, 256 b + 256). Its tile is the contiguous range
-   [tile_ptr[b], tile_ptr[b] + tile_count[b]) of the tile_* arrays: first the
-   edges whose left cell is in b (the reference's resident edge order,
-   gpu_resident_batch.py:175), then the edges whose right cell is in b and
-   left cell is not. lcsr[k] = (position in the tile << 1) | is_right for
-   the CSR slots k of each cell, in the reference's per-cell order
-   (inundation/mesh/geometry.py:454-468, remapped as blocks.py:33-44). */
+   [tile_ptr[b], tile_ptr[b + 1]) of the tile_* arrays, tile_count[b] records
+   and then padding to a multiple of 32: first the edges whose left cell is
+   in b (the reference's resident edge order, gpu_resident_batch.py:175), then
+   the edges whose right cell is in b and left cell is not.
+   lcsr[k] = (position in the tile << 1) | is_right for the CSR slots k of each
+   cell, in the reference's per-cell order (inundation/mesh/geometry.py:454-468,
+   remapped as blocks.py:33-44); lcsr_blk holds the same entries regrouped per
+   block, block b's from lcsr_blk[lcsr_ptr[b]] (a multiple of 8).
+   Every per-cell array (area, n_mann and all state arrays) holds
+   n_blocks * 256 entries; cptr holds n_blocks * 256 + 4, repeating the total
+   past n_cells. These paddings let whole blocks be bulk-copied. */
 typedef struct {
     uint32_t n_cells;
     uint32_t n_blocks;
     uint32_t max_tile_edges;  /* the largest tile_count */
-    uint32_t pad0;
+    uint32_t max_block_slots; /* the largest lcsr_ptr[b + 1] - lcsr_ptr[b] */
     const int32_t *tile_cl;   /* left cell */
     const int32_t *tile_cr;   /* right cell, -1 on a wall */
     const float *tile_nx;
@@ -66,14 +71,16 @@ typedef struct {
     const float *tile_len;
     const float *tile_dzl;    /* face elevation minus the left bed */
     const float *tile_dzr;
-    const uint32_t *tile_ptr;   /* n_blocks */
+    const uint32_t *tile_ptr;   /* n_blocks + 1 */
     const uint32_t *tile_count; /* n_blocks */
-    const uint32_t *cptr;       /* n_cells + 1 */
+    const uint32_t *cptr;       /* n_blocks * 256 + 4 */
     const uint16_t *lcsr;       /* cptr[n_cells] */
     const float *area;
     const float *n_mann;
     const uint32_t *ring_ptr;   /* block two-ring CSR (blocks.py:93-118) */
     const uint32_t *ring_idx;
+    const uint16_t *lcsr_blk;
+    const uint32_t *lcsr_ptr;   /* n_blocks + 1 */
 } swe_mesh_t;
 
 /* Mutable state and the per-run workspace (device pointers). */
@@ -83,7 +90,8 @@ typedef struct {
     float *clamp_mass;             /* per-cell positivity-clamp volume (diagnostic) */
     uint32_t *blk;                 /* 3 words per block: wet, active, forced */
     uint32_t *active_list;         /* n_blocks: active blocks of the current step */
-    uint32_t *sched;               /* 8 words: [0] active count, [1] next count, [2] done CTAs, [3] active blocks computed */
+    uint32_t *sched;               /* 8 words: [0] active count, [1] next count, [2] done CTAs, [3] cells of the
+                                      active blocks, [4] next cells, [6..7] uint64 cells computed over real steps */
     uint32_t *dt_buf;              /* [0] this step's dt (float bits, 0 = no-op), [1] next CFL bound */
     swe_ctrl_t *ctrl;
 } swe_state_t;
@@ -96,7 +104,7 @@ typedef struct {
     uint32_t track_clamp; /* accumulate the clamp diagnostic */
     uint32_t active_set;  /* skip blocks outside the two-ring of wet blocks */
     uint32_t grid;        /* CTAs of the persistent per-block kernels (0 = one per block) */
-    uint32_t pad;
+    uint32_t kernel;      /* stage kernel: 0 = bulk-copy staged tiles (default), 1 = plain loads */
 } swe_params_t;
 
 /* Sparse sources: n pairs (cell, dh/dt) on the device. */
@@ -113,8 +121,10 @@ size_t swe_workspace_bytes(uint32_t n_cells);
 /* Dynamic shared memory one per-block CTA needs for a tile of max_tile_edges. */
 size_t swe_tile_smem_bytes(uint32_t max_tile_edges);
 
-/* Persistent CTAs per SM for the per-block kernels at that tile size (occupancy query). */
-int swe_blocks_per_sm(uint32_t max_tile_edges, int *out);
+/* Sets the shared-memory size of every per-block kernel for this mesh (call
+   once, before any stream capture) and returns the persistent CTAs per SM of
+   the chosen stage kernel (0 staged, 1 plain). */
+int swe_configure(const swe_mesh_t *mesh, int kernel, int *blocks_per_sm);
 
 /* One Heun stage over the active blocks, fused: edge fluxes of each block's
    tile into shared memory, the fixed-order per-cell gather and the update.

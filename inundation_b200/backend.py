@@ -55,7 +55,7 @@ RESIDENT_CTRL_DTYPE = np.dtype(
         ("dry_dt_ticks", "<u4"),
         ("last_raw", "<f4"),
         ("cfl_safety", "<f4"),
-        ("_pad", "<u4"),
+        ("error", "<u4"),
     ]
 )
 
@@ -78,6 +78,8 @@ class SWESolverB200Resident:
     deterministic: bool = True
     compensated: bool = True
     cfl_safety: float = 1.0
+    # Stage kernel: "staged" (bulk-copied tiles, double-buffered) or "plain" (direct loads).
+    stage_kernel: str = "staged"
 
     def __init__(
         self,
@@ -154,25 +156,37 @@ class SWESolverB200Resident:
             "cptr": self._dev(_i32(L.cptr)),
             "lcsr": self._dev(L.lcsr.view(np.int16)),
             "area": self._dev(L.area),
-            "n_mann": self._dev(n0),
+            "n_mann": self._dev(np.concatenate([n0, np.full(L.n_padded_cells - L.n_cells, 0.03, np.float32)])),
             "ring_ptr": self._dev(_i32(L.ring_ptr)),
             "ring_idx": self._dev(_i32(L.ring_idx)),
+            "lcsr_blk": self._dev(L.lcsr_blk.view(np.int16)),
+            "lcsr_ptr": self._dev(_i32(L.lcsr_ptr)),
         }
         self._mesh_t = t
         m = native.SweMesh()
         m.n_cells = L.n_cells
         m.n_blocks = L.n_blocks
         m.max_tile_edges = L.max_tile_edges
+        m.max_block_slots = L.max_block_slots
         for name, tensor in t.items():
             setattr(m, name, tensor.data_ptr())
         self._mesh = m
-        per_sm = ctypes.c_int(0)
-        native.check(self._lib.swe_blocks_per_sm(L.max_tile_edges, ctypes.byref(per_sm)), "occupancy query")
-        sms = torch.cuda.get_device_properties(self.device).multi_processor_count
-        self._grid = max(1, min(L.n_blocks, per_sm.value * sms))
+        self._sms = torch.cuda.get_device_properties(self.device).multi_processor_count
+        self._grids: dict[int, int] = {}
+        for kernel in (0, 1):
+            per_sm = ctypes.c_int(0)
+            with torch.cuda.device(self.device):
+                native.check(self._lib.swe_configure(ctypes.byref(m), kernel, ctypes.byref(per_sm)), "swe_configure")
+            self._grids[kernel] = max(1, min(L.n_blocks, per_sm.value * self._sms))
+
+    @property
+    def _kernel(self) -> int:
+        if self.stage_kernel not in ("staged", "plain"):
+            raise ValueError(f"stage_kernel must be 'staged' or 'plain', got {self.stage_kernel!r}")
+        return 0 if self.stage_kernel == "staged" else 1
 
     def _alloc_state(self) -> None:
-        n, nb, dev = self.N, self.n_blocks, self.device
+        n, nb, dev = self.layout.n_padded_cells, self.n_blocks, self.device
         z = lambda: torch.zeros(n, dtype=torch.float32, device=dev)  # noqa: E731
         self._t = {name: z() for name in ("h", "hu", "hv", "h_lo", "h1", "hu1", "hv1", "h1_lo", "clamp_mass")}
         self._blk = torch.zeros(3 * nb, dtype=torch.int32, device=dev)
@@ -202,7 +216,8 @@ class SWESolverB200Resident:
             compensated=int(bool(self.compensated)),
             track_clamp=int(bool(self.track_clamp)),
             active_set=int(bool(self.active_set)),
-            grid=self._grid,
+            grid=self._grids[self._kernel],
+            kernel=self._kernel,
         )
 
     def _sources(self) -> native.SweSources:
@@ -217,7 +232,7 @@ class SWESolverB200Resident:
     # -- public state access (reference solver.py:390-497) --------------------------------------
     def _download(self, tensor: torch.Tensor) -> NDArray[np.float32]:
         with torch.cuda.stream(self._stream):
-            out = tensor.cpu().numpy()
+            out = tensor[: self.N].cpu().numpy()
         return out.copy()
 
     def download_h(self) -> NDArray[np.float32]:
@@ -240,7 +255,9 @@ class SWESolverB200Resident:
 
     def download_block_flags(self) -> NDArray[np.uint32]:
         """``(n_blocks, 3)`` flags: wet, active, forced."""
-        return self._download(self._blk).view(np.uint32).reshape(self.n_blocks, 3).copy()
+        with torch.cuda.stream(self._stream):
+            words = self._blk.cpu().numpy()
+        return words.view(np.uint32).reshape(self.n_blocks, 3).copy()
 
     def reset_clamp_mass(self) -> None:
         with torch.cuda.stream(self._stream):
@@ -250,7 +267,7 @@ class SWESolverB200Resident:
         """Overwrite one state array (``h``, ``hu``, ``hv``, ``h1``, ...) on the device."""
         src = torch.from_numpy(np.ascontiguousarray(values, np.float32).ravel())
         with torch.cuda.stream(self._stream):
-            self._t[name].copy_(src)
+            self._t[name][: self.N].copy_(src)
         self._stream.synchronize()
 
     def reset(self, h0: NDArray[np.float32], hu0: NDArray[np.float32], hv0: NDArray[np.float32]) -> None:
@@ -259,9 +276,9 @@ class SWESolverB200Resident:
         self._hu0 = np.asarray(hu0, np.float32).ravel().copy()
         self._hv0 = np.asarray(hv0, np.float32).ravel().copy()
         with torch.cuda.stream(self._stream):
-            self._t["h"].copy_(torch.from_numpy(self._h0))
-            self._t["hu"].copy_(torch.from_numpy(self._hu0))
-            self._t["hv"].copy_(torch.from_numpy(self._hv0))
+            self._t["h"][: self.N].copy_(torch.from_numpy(self._h0))
+            self._t["hu"][: self.N].copy_(torch.from_numpy(self._hu0))
+            self._t["hv"][: self.N].copy_(torch.from_numpy(self._hv0))
             self._t["h_lo"].zero_()
             self._t["h1_lo"].zero_()
         self._stream.synchronize()
@@ -325,6 +342,10 @@ class SWESolverB200Resident:
         with torch.cuda.stream(self._stream):
             self._ctrl_pinned.copy_(self._ctrl_dev, non_blocking=True)
         self._stream.synchronize()
+        if int(self._ctrl["error"][0]):
+            raise RuntimeError(
+                f"{B200_BACKEND}: a bounded device wait for staged data timed out (error {int(self._ctrl['error'][0])})"
+            )
 
     def _enqueue_prologue(self) -> None:
         p = self._params()
@@ -357,6 +378,7 @@ class SWESolverB200Resident:
             bool(self.compensated),
             bool(self.track_clamp),
             bool(self.active_set),
+            self._kernel,
             self._src_count,
             self._src_cells.data_ptr(),
             self._src_rate.data_ptr(),
@@ -429,6 +451,7 @@ class SWESolverB200Resident:
 
         capture()
         ctrl = self._ctrl
+        ctrl["error"] = 0
         ctrl["now_ticks"] = start_ticks
         ctrl["steps"] = 0
         ctrl["dt_ticks"] = 0

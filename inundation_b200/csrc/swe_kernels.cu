@@ -248,6 +248,392 @@ __global__ void __launch_bounds__(kThreads) stage_kernel(swe_mesh_t m, swe_state
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// Bulk copies (TMA, 1-D, no multicast) into shared memory, completed on an
+// mbarrier; every wait is bounded by a deadline on the global timer.
+// ---------------------------------------------------------------------------
+constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s
+constexpr int kStageThreads = 512;
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_barrier_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return done != 0u;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// True once the barrier's phase of this parity completed; false after the deadline.
+__device__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    if (mbar_test(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    while (!mbar_test(bar, parity)) {
+        if (global_ns() - t0 > kWaitLimitNs) return false;
+    }
+    return true;
+}
+
+// Shared-memory plan of the staged stage kernel: two buffers, each holding a
+// block's tile (7 arrays of capE), its cell data (nc arrays of 256), its
+// cptr window (260 words) and its local CSR (capS halfwords), then the
+// per-cell velocities of the block being computed.
+struct StagePlan {
+    uint32_t capE, capS, nc, buf_bytes, off_vel, total;
+};
+
+__host__ __device__ inline StagePlan stage_plan(uint32_t max_tile_edges, uint32_t max_block_slots, uint32_t nc) {
+    StagePlan L;
+    L.capE = (max_tile_edges + 31u) & ~31u;
+    L.capS = (max_block_slots + 63u) & ~63u;
+    L.nc = nc;
+    L.buf_bytes = 7u * L.capE * 4u + nc * 1024u + 1152u + L.capS * 2u;
+    L.off_vel = 128u + 2u * L.buf_bytes;
+    L.total = L.off_vel + 2u * 256u * 4u;
+    return L;
+}
+
+struct StageBuf {
+    int32_t *cl, *cr;
+    float *nx, *ny, *len, *dzl, *dzr;
+    float *c;          // nc x 256: [0..3] the stage's input state, [4] area, [5] n, [6..9] committed state (stage 1)
+    uint32_t *cptr;    // 260
+    uint16_t *lcsr;    // capS
+    uint64_t *bar;
+};
+
+__device__ __forceinline__ StageBuf stage_buf(unsigned char *smem, const StagePlan &L, uint32_t k) {
+    unsigned char *base = smem + 128u + k * L.buf_bytes;
+    StageBuf B;
+    const uint32_t e = L.capE * 4u;
+    B.cl = reinterpret_cast<int32_t *>(base);
+    B.cr = reinterpret_cast<int32_t *>(base + e);
+    B.nx = reinterpret_cast<float *>(base + 2u * e);
+    B.ny = reinterpret_cast<float *>(base + 3u * e);
+    B.len = reinterpret_cast<float *>(base + 4u * e);
+    B.dzl = reinterpret_cast<float *>(base + 5u * e);
+    B.dzr = reinterpret_cast<float *>(base + 6u * e);
+    B.c = reinterpret_cast<float *>(base + 7u * e);
+    B.cptr = reinterpret_cast<uint32_t *>(base + 7u * e + L.nc * 1024u);
+    B.lcsr = reinterpret_cast<uint16_t *>(base + 7u * e + L.nc * 1024u + 1152u);
+    B.bar = reinterpret_cast<uint64_t *>(smem) + k;
+    return B;
+}
+
+// Warp 0 stages block b into buffer B: one bulk copy per lane.
+template <int STAGE>
+__device__ void stage_issue(const swe_mesh_t &m, const swe_state_t &s, uint32_t b, const StageBuf &B) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t e0 = m.tile_ptr[b], ep = m.tile_ptr[b + 1] - e0;
+    const uint32_t l0 = m.lcsr_ptr[b], lp = m.lcsr_ptr[b + 1] - l0;
+    const uint32_t c0 = b * kBlockCells;
+    constexpr uint32_t nc = STAGE ? 10u : 6u;
+    if (lane == 0) mbar_expect_tx(B.bar, 7u * ep * 4u + nc * 1024u + 1040u + lp * 2u);
+    __syncwarp();
+    if (lane < 7u) {
+        const void *src;
+        void *dst;
+        switch (lane) {
+            case 0: src = m.tile_cl; dst = B.cl; break;
+            case 1: src = m.tile_cr; dst = B.cr; break;
+            case 2: src = m.tile_nx; dst = B.nx; break;
+            case 3: src = m.tile_ny; dst = B.ny; break;
+            case 4: src = m.tile_len; dst = B.len; break;
+            case 5: src = m.tile_dzl; dst = B.dzl; break;
+            default: src = m.tile_dzr; dst = B.dzr; break;
+        }
+        bulk_load(dst, static_cast<const char *>(src) + 4ull * e0, ep * 4u, B.bar);
+    } else if (lane < 7u + nc) {
+        const uint32_t k = lane - 7u;
+        const float *src;
+        switch (k) {
+            case 0: src = STAGE ? s.h1 : s.h; break;
+            case 1: src = STAGE ? s.hu1 : s.hu; break;
+            case 2: src = STAGE ? s.hv1 : s.hv; break;
+            case 3: src = STAGE ? s.h1_lo : s.h_lo; break;
+            case 4: src = m.area; break;
+            case 5: src = m.n_mann; break;
+            case 6: src = s.h; break;
+            case 7: src = s.hu; break;
+            case 8: src = s.hv; break;
+            default: src = s.h_lo; break;
+        }
+        bulk_load(B.c + k * 256u, src + c0, 1024u, B.bar);
+    } else if (lane == 7u + nc) {
+        bulk_load(B.cptr, m.cptr + c0, 1040u, B.bar);
+    } else if (lane == 8u + nc && lp != 0u) {
+        bulk_load(B.lcsr, m.lcsr_blk + l0, lp * 2u, B.bar);
+    }
+}
+
+__device__ __forceinline__ uint32_t block_min_any(uint32_t v, uint32_t *scratch) {
+    v = __reduce_min_sync(0xFFFFFFFFu, v);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    if (lane == 0) scratch[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = (lane < nw) ? scratch[lane] : kNoBound;
+        w = __reduce_min_sync(0xFFFFFFFFu, w);
+        if (lane == 0) scratch[0] = w;
+    }
+    __syncthreads();
+    const uint32_t r = scratch[0];
+    __syncthreads();
+    return r;
+}
+
+// HLLC with the face-frame velocities of the reconstructed states, written
+// without divergent branches: the star state of the side the contact wave
+// leaves behind is formed once. Same expressions as hllc(), bit for bit.
+__device__ __forceinline__ void hllc_select(const Phys &p, float hL, float hqnL, float hqtL, float hR, float hqnR,
+                                            float hqtR, float &Fh, float &Fhn, float &Fht, float &smax) {
+    const float unL = safe_vel(p, hL, hqnL), utL = safe_vel(p, hL, hqtL);
+    const float unR = safe_vel(p, hR, hqnR), utR = safe_vel(p, hR, hqtR);
+    float SL, SR;
+    hllc_speeds_fast(p, hL, unL, hR, unR, SL, SR);
+    smax = gmax(fabsf(SL), fabsf(SR));
+    const float num_sm = SL * hR * (unR - SR) - SR * hL * (unL - SL);
+    const float den_sm = hR * (unR - SR) - hL * (unL - SL);
+    const float SM = (fabsf(den_sm) > 1e-12f) ? num_sm / den_sm : 0.0f;
+    const float FLh = hL * unL, FLn = hL * unL * unL + 0.5f * p.g * hL * hL, FLt = hL * unL * utL;
+    const float FRh = hR * unR, FRn = hR * unR * unR + 0.5f * p.g * hR * hR, FRt = hR * unR * utR;
+    const bool left = SM >= 0.0f;
+    const float hK = left ? hL : hR, unK = left ? unL : unR, utK = left ? utL : utR, SK = left ? SL : SR;
+    const float FKh = left ? FLh : FRh, FKn = left ? FLn : FRn, FKt = left ? FLt : FRt;
+    const float dSK = SK - SM;
+    const float kK = hK * (SK - unK) / ((fabsf(dSK) > 1e-14f) ? dSK : 1e-14f);
+    const float Fsh = FKh + SK * (kK - hK);
+    const float Fsn = FKn + SK * (kK * SM - hK * unK);
+    const float Fst = FKt + SK * (kK * utK - hK * utK);
+    const bool useL = SL >= 0.0f, useR = !useL && !left && !(SR >= 0.0f);
+    Fh = useL ? FLh : (useR ? FRh : Fsh);
+    Fhn = useL ? FLn : (useR ? FRn : Fsn);
+    Fht = useL ? FLt : (useR ? FRt : Fst);
+}
+
+// ---------------------------------------------------------------------------
+// One Heun stage over the active blocks, staged: each CTA prefetches its next
+// block (tile, cell data, cptr window, local CSR) with bulk copies while it
+// computes the current one. Same arithmetic as stage_kernel, bit for bit.
+// ---------------------------------------------------------------------------
+template <int STAGE, bool COMP, bool CLAMP>
+__global__ void __launch_bounds__(kStageThreads, 2) stage_staged_kernel(swe_mesh_t m, swe_state_t s, Phys p, float cfl) {
+    const uint32_t dt_bits = s.dt_buf[0];
+    if (dt_bits == 0u) return;
+    const uint32_t count = s.sched[kSchedActive];
+    if (blockIdx.x >= count) return;
+    const float dt = __uint_as_float(dt_bits);
+    constexpr uint32_t nc = STAGE ? 10u : 6u;
+    const StagePlan L = stage_plan(m.max_tile_edges, m.max_block_slots, nc);
+    extern __shared__ __align__(128) unsigned char smem[];
+    float *su = reinterpret_cast<float *>(smem + L.off_vel);
+    float *sv = su + 256;
+    __shared__ uint32_t red[kStageThreads / 32];
+    const uint32_t tid = threadIdx.x;
+    if (tid == 0) {
+        mbar_init(reinterpret_cast<uint64_t *>(smem), 1u);
+        mbar_init(reinterpret_cast<uint64_t *>(smem) + 1, 1u);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (tid < 32u) stage_issue<STAGE>(m, s, s.active_list[blockIdx.x], stage_buf(smem, L, 0));
+
+    uint32_t it = 0;
+    for (uint32_t w = blockIdx.x; w < count; w += gridDim.x, ++it) {
+        const uint32_t b = s.active_list[w];
+        const StageBuf B = stage_buf(smem, L, it & 1u);
+        const uint32_t wn = w + gridDim.x;
+        if (tid < 32u && wn < count) stage_issue<STAGE>(m, s, s.active_list[wn], stage_buf(smem, L, (it + 1u) & 1u));
+        const bool ok = mbar_wait(B.bar, (it >> 1) & 1u);
+        if (!__syncthreads_and(ok)) {
+            // The staged data never arrived: report it, let any prefetch land, stop.
+            if (tid == 0) atomicOr(&s.ctrl->error, 1u);
+            if (wn < count) mbar_wait(stage_buf(smem, L, (it + 1u) & 1u).bar, ((it + 1u) >> 1) & 1u);
+            return;
+        }
+        const float *C0 = B.c, *C1 = B.c + 256, *C2 = B.c + 512;
+        const int base = static_cast<int>(b * kBlockCells);
+        if (tid < 256u) {
+            su[tid] = safe_vel(p, C0[tid], C1[tid]);
+            sv[tid] = safe_vel(p, C0[tid], C2[tid]);
+        }
+        __syncthreads();
+
+        // Edge fluxes of the tile, written in place over the consumed records.
+        const uint32_t ne = m.tile_count[b];
+        for (uint32_t j = tid; j < ne; j += kStageThreads) {
+            const int cL = B.cl[j], cR = B.cr[j];
+            const float nx = B.nx[j], ny = B.ny[j];
+            float hL, huL, hvL, uL, vL, hR, huR, hvR, uR, vR;
+            const uint32_t lL = static_cast<uint32_t>(cL - base);
+            if (lL < 256u) {
+                hL = C0[lL]; huL = C1[lL]; hvL = C2[lL]; uL = su[lL]; vL = sv[lL];
+            } else {
+                load_state<STAGE>(s, cL, hL, huL, hvL);
+                uL = safe_vel(p, hL, huL);
+                vL = safe_vel(p, hL, hvL);
+            }
+            if (cR < 0) {
+                hR = hL;
+                wall_mirror(huL, hvL, nx, ny, huR, hvR);
+                uR = safe_vel(p, hR, huR);
+                vR = safe_vel(p, hR, hvR);
+            } else {
+                const uint32_t lR = static_cast<uint32_t>(cR - base);
+                if (lR < 256u) {
+                    hR = C0[lR]; huR = C1[lR]; hvR = C2[lR]; uR = su[lR]; vR = sv[lR];
+                } else {
+                    load_state<STAGE>(s, cR, hR, huR, hvR);
+                    uR = safe_vel(p, hR, huR);
+                    vR = safe_vel(p, hR, hvR);
+                }
+            }
+            const bool live = !(hL < p.dry_tol && hR < p.dry_tol);
+            B.cr[j] = live ? 1 : 0;
+            if (!live) continue;
+            const float len = B.len[j], dzL = B.dzl[j], dzR = B.dzr[j];
+            const float hLs = gmax(0.0f, hL - dzL), hRs = gmax(0.0f, hR - dzR);
+            const float huLs = hLs * uL, hvLs = hLs * vL, huRs = hRs * uR, hvRs = hRs * vR;
+            const float hqnL = huLs * nx + hvLs * ny, hqtL = -huLs * ny + hvLs * nx;
+            const float hqnR = huRs * nx + hvRs * ny, hqtR = -huRs * ny + hvRs * nx;
+            float Fh, Fhn, Fht, smax;
+            hllc_select(p, hLs, hqnL, hqtL, hRs, hqnR, hqtR, Fh, Fhn, Fht, smax);
+            if (cR < 0) Fh = 0.0f;  // a wall passes no mass
+            const float Fhu = Fhn * nx - Fht * ny;
+            const float Fhv = Fhn * ny + Fht * nx;
+            const float SL_g = 0.5f * p.g * (hL * hL - hLs * hLs);
+            const float SR_g = 0.5f * p.g * (hR * hR - hRs * hRs);
+            B.nx[j] = Fh * len;
+            B.ny[j] = Fhu * len + SL_g * nx * len;
+            B.len[j] = Fhv * len + SL_g * ny * len;
+            B.dzl[j] = Fhu * len + SR_g * nx * len;
+            B.dzr[j] = Fhv * len + SR_g * ny * len;
+            if (STAGE == 1) B.cl[j] = __float_as_int(smax * len);
+        }
+        __syncthreads();
+
+        const uint32_t i = b * kBlockCells + tid;
+        bool wet = false;
+        uint32_t bound = kNoBound;
+        if (tid < 256u && i < m.n_cells) {
+            const float A = B.c[4 * 256 + tid];
+            const float dti = dt / A;
+            const float hi = C0[tid], hui = C1[tid], hvi = C2[tid];
+            float sdh = 0.0f, sdhu = 0.0f, sdhv = 0.0f, lam = 0.0f;
+            const uint32_t k0 = B.cptr[tid] - B.cptr[0], k1 = B.cptr[tid + 1] - B.cptr[0];
+            for (uint32_t k = k0; k < k1; ++k) {
+                const uint32_t v = B.lcsr[k];
+                const uint32_t j = v >> 1;
+                if (!B.cr[j]) continue;
+                if (v & 1u) {
+                    sdh -= B.nx[j];
+                    sdhu -= B.dzl[j];
+                    sdhv -= B.dzr[j];
+                } else {
+                    sdh += B.nx[j];
+                    sdhu += B.ny[j];
+                    sdhv += B.len[j];
+                }
+                if (STAGE == 1) lam += __int_as_float(B.cl[j]);
+            }
+            float h_new, lo_new, h_raw;
+            if (COMP) {
+                const float loi = B.c[3 * 256 + tid];
+                add_compensated(hi, loi, -dti * sdh, h_new, lo_new);
+                float s_raw, e_raw;
+                two_sum(hi, -dti * sdh, s_raw, e_raw);
+                h_raw = s_raw + (e_raw + loi);
+            } else {
+                h_raw = hi - dti * sdh;
+                h_new = gmax(h_raw, 0.0f);
+                lo_new = 0.0f;
+            }
+            float hu_new = hui - dti * sdhu;
+            float hv_new = hvi - dti * sdhv;
+            if (CLAMP) s.clamp_mass[i] += 0.5f * A * (h_new - h_raw);
+            if (h_new < p.dry_tol) {
+                hu_new = 0.0f;
+                hv_new = 0.0f;
+            }
+            if (h_new >= p.dry_tol) {
+                const float drag = film_drag(p, h_new, dt);
+                hu_new *= drag;
+                hv_new *= drag;
+                const float n = B.c[5 * 256 + tid];
+                const float u_ = hu_new / h_new, v_ = hv_new / h_new;
+                const float spd = sqrtf(u_ * u_ + v_ * v_);
+                const float Sf = p.g * n * n * spd / pow43(h_new);
+                const float den = 1.0f + dt * Sf;
+                hu_new = hu_new / den;
+                hv_new = hv_new / den;
+            }
+            if (STAGE == 0) {
+                s.h1[i] = h_new;
+                if (COMP) s.h1_lo[i] = lo_new;
+                s.hu1[i] = hu_new;
+                s.hv1[i] = hv_new;
+            } else {
+                const float h0 = B.c[6 * 256 + tid], hu0 = B.c[7 * 256 + tid], hv0 = B.c[8 * 256 + tid];
+                float hf;
+                if (COMP) {
+                    float sm, em, lof;
+                    two_sum(h0, h_new, sm, em);
+                    em += B.c[9 * 256 + tid] + lo_new;
+                    two_sum(0.5f * sm, 0.5f * em, hf, lof);
+                    s.h_lo[i] = lof;
+                } else {
+                    hf = 0.5f * (h0 + h_new);
+                }
+                s.h[i] = hf;
+                float huf = 0.5f * (hu0 + hu_new);
+                float hvf = 0.5f * (hv0 + hv_new);
+                if (hf < p.dry_tol) {
+                    huf = 0.0f;
+                    hvf = 0.0f;
+                }
+                s.hu[i] = huf;
+                s.hv[i] = hvf;
+                wet = hf >= p.dry_tol;
+                if (lam > 1e-30f && A > 1e-10f) bound = __float_as_uint(cfl * A / lam);
+            }
+        }
+        if (STAGE == 1) {
+            const int any_wet = __syncthreads_or(wet);
+            const uint32_t bmin = block_min_any(bound, red);
+            if (tid == 0) {
+                s.blk[kBlkWords * b + kBlkWet] = any_wet ? 1u : 0u;
+                if (bmin != kNoBound) atomicMin(&s.dt_buf[1], bmin);
+            }
+        }
+        // This buffer is refilled by bulk copies two iterations on.
+        fence_proxy_async();
+        __syncthreads();
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Integer-tick step control (resident.py:813-885).
 // ---------------------------------------------------------------------------
@@ -526,7 +912,7 @@ inline int check_launch() { return cudaGetLastError() == cudaSuccess ? SWE_OK : 
 inline bool mesh_ok(const swe_mesh_t *m) {
     return m && m->n_cells && m->n_blocks && m->tile_cl && m->tile_cr && m->tile_nx && m->tile_ny && m->tile_len &&
            m->tile_dzl && m->tile_dzr && m->tile_ptr && m->tile_count && m->cptr && m->lcsr && m->area &&
-           m->n_mann && m->ring_ptr && m->ring_idx;
+           m->n_mann && m->ring_ptr && m->ring_idx && m->lcsr_blk && m->lcsr_ptr;
 }
 
 inline bool state_ok(const swe_state_t *s) {
@@ -549,12 +935,28 @@ inline uint32_t grid_of(const swe_mesh_t *m, const swe_params_t *p) {
 
 template <int STAGE, bool COMP, bool CLAMP>
 int launch_stage(const swe_mesh_t *m, const swe_state_t *s, const swe_params_t *p, cudaStream_t st) {
-    auto kern = stage_kernel<STAGE, COMP, CLAMP>;
-    const size_t bytes = tile_smem_bytes(m->max_tile_edges);
+    if (p->kernel == 1u) {
+        auto kern = stage_kernel<STAGE, COMP, CLAMP>;
+        const size_t bytes = tile_smem_bytes(m->max_tile_edges);
+        int rc = set_smem(kern, bytes);
+        if (rc) return rc;
+        kern<<<grid_of(m, p), kThreads, bytes, st>>>(*m, *s, Phys{p->g, p->dry_tol}, p->cfl);
+        return check_launch();
+    }
+    auto kern = stage_staged_kernel<STAGE, COMP, CLAMP>;
+    const size_t bytes = stage_plan(m->max_tile_edges, m->max_block_slots, STAGE ? 10u : 6u).total;
     int rc = set_smem(kern, bytes);
     if (rc) return rc;
-    kern<<<grid_of(m, p), kThreads, bytes, st>>>(*m, *s, Phys{p->g, p->dry_tol}, p->cfl);
+    kern<<<grid_of(m, p), kStageThreads, bytes, st>>>(*m, *s, Phys{p->g, p->dry_tol}, p->cfl);
     return check_launch();
+}
+
+template <int STAGE, bool COMP, bool CLAMP>
+int configure_stage(const swe_mesh_t *m) {
+    int rc = set_smem(stage_kernel<STAGE, COMP, CLAMP>, tile_smem_bytes(m->max_tile_edges));
+    if (rc) return rc;
+    return set_smem(stage_staged_kernel<STAGE, COMP, CLAMP>,
+                    stage_plan(m->max_tile_edges, m->max_block_slots, STAGE ? 10u : 6u).total);
 }
 
 template <int STAGE>
@@ -578,14 +980,28 @@ size_t swe_workspace_bytes(uint32_t n_cells) {
 
 size_t swe_tile_smem_bytes(uint32_t max_tile_edges) { return tile_smem_bytes(max_tile_edges); }
 
-int swe_blocks_per_sm(uint32_t max_tile_edges, int *out) {
-    if (!out) return SWE_ERR_ARGUMENT;
-    const size_t bytes = tile_smem_bytes(max_tile_edges);
-    auto kern = stage_kernel<1, true, false>;
-    int rc = set_smem(kern, bytes);
+int swe_configure(const swe_mesh_t *mesh, int kernel, int *blocks_per_sm) {
+    if (!mesh_ok(mesh) || !blocks_per_sm || kernel < 0 || kernel > 1) return SWE_ERR_ARGUMENT;
+    int rc = configure_stage<0, false, false>(mesh);
+    if (!rc) rc = configure_stage<0, false, true>(mesh);
+    if (!rc) rc = configure_stage<0, true, false>(mesh);
+    if (!rc) rc = configure_stage<0, true, true>(mesh);
+    if (!rc) rc = configure_stage<1, false, false>(mesh);
+    if (!rc) rc = configure_stage<1, false, true>(mesh);
+    if (!rc) rc = configure_stage<1, true, false>(mesh);
+    if (!rc) rc = configure_stage<1, true, true>(mesh);
+    if (!rc) rc = set_smem(cfl_prologue_kernel, tile_smem_bytes(mesh->max_tile_edges));
     if (rc) return rc;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, kern, kThreads, bytes) != cudaSuccess) return SWE_ERR_CUDA;
-    return SWE_OK;
+    cudaError_t err;
+    if (kernel == 1) {
+        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, stage_kernel<1, true, false>, kThreads,
+                                                            tile_smem_bytes(mesh->max_tile_edges));
+    } else {
+        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            blocks_per_sm, stage_staged_kernel<1, true, false>, kStageThreads,
+            stage_plan(mesh->max_tile_edges, mesh->max_block_slots, 10u).total);
+    }
+    return err == cudaSuccess ? SWE_OK : SWE_ERR_CUDA;
 }
 
 int swe_stage(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params_t *params, int stage, swe_stream_t stream) {

@@ -61,6 +61,36 @@ __device__ __forceinline__ void hllc_speeds(const Phys &p, float hL, float unL, 
     SRo = roe * SR + dryLeft * (unR + cR) + dryRight * (unL + 2.0f * cL);
 }
 
+// clamp(h / dry_tol - 1, 0, 1) without the division where its value is known:
+// division is correctly rounded and monotone, so h >= 2 dry_tol gives exactly
+// 1 and h <= dry_tol exactly +0. NaN falls through to the full expression.
+__device__ __forceinline__ float wet_blend(const Phys &p, float h) {
+    if (h >= 2.0f * p.dry_tol) return 1.0f;
+    if (h <= p.dry_tol) return 0.0f;
+    return gclamp(h / p.dry_tol - 1.0f, 0.0f, 1.0f);
+}
+
+// hllc_speeds with wet_blend for the two blend weights: the same values, bit for bit.
+__device__ __forceinline__ void hllc_speeds_fast(const Phys &p, float hL, float unL, float hR, float unR, float &SLo,
+                                                 float &SRo) {
+    const float cL = sqrtf(p.g * gmax(hL, 0.0f));
+    const float cR = sqrtf(p.g * gmax(hR, 0.0f));
+    const float sqL = sqrtf(gmax(hL, 0.0f));
+    const float sqR = sqrtf(gmax(hR, 0.0f));
+    const float den = sqL + sqR;
+    const float u_roe = (den > 1e-12f) ? (sqL * unL + sqR * unR) / den : 0.0f;
+    const float c_roe = sqrtf(p.g * 0.5f * (hL + hR));
+    const float SL = gmin(unL - cL, u_roe - c_roe);
+    const float SR = gmax(unR + cR, u_roe + c_roe);
+    const float wetL = wet_blend(p, hL);
+    const float wetR = wet_blend(p, hR);
+    const float dryLeft = (1.0f - wetL) * wetR;
+    const float dryRight = (1.0f - wetR) * wetL;
+    const float roe = 1.0f - dryLeft - dryRight;
+    SLo = roe * SL + dryLeft * (unR - 2.0f * cR) + dryRight * (unL - cL);
+    SRo = roe * SR + dryLeft * (unR + cR) + dryRight * (unL + 2.0f * cL);
+}
+
 // HLLC flux in the face frame (Toro 2001); smax is the largest speed assumed.
 __device__ __forceinline__ void hllc(const Phys &p, float hL, float hqnL, float hqtL, float hR, float hqnR,
                                      float hqtR, float &Fh, float &Fhn, float &Fht, float &smax) {

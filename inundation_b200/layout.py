@@ -46,14 +46,21 @@ class TileLayout:
     tile_len: NDArray[np.float32]
     tile_dzl: NDArray[np.float32]
     tile_dzr: NDArray[np.float32]
-    tile_ptr: NDArray[np.uint32]
+    tile_ptr: NDArray[np.uint32]  # n_blocks + 1: tile b is [tile_ptr[b], tile_ptr[b + 1]) with padding
     tile_count: NDArray[np.uint32]
     tile_edge: NDArray[np.int64]  # resident edge id of every tile record (-1 on padding)
-    cptr: NDArray[np.uint32]
+    cptr: NDArray[np.uint32]  # n_blocks * 256 + 4 entries; past n_cells they repeat the total
     lcsr: NDArray[np.uint16]
+    lcsr_blk: NDArray[np.uint16]  # lcsr regrouped per block, block b's slots from lcsr_ptr[b]
+    lcsr_ptr: NDArray[np.uint32]  # n_blocks + 1, multiples of 8 (16-byte aligned segments)
+    max_block_slots: int  # the largest padded slot segment of a block
     ring_ptr: NDArray[np.uint32]
     ring_idx: NDArray[np.uint32]
     area: NDArray[np.float32]
+
+    @property
+    def n_padded_cells(self) -> int:
+        return self.n_blocks * ACTIVE_BLOCK_CELLS
 
     @property
     def n_tile_records(self) -> int:
@@ -121,6 +128,18 @@ def build_tile_layout(geom: MeshGeometry) -> TileLayout:
         raise ValueError("local tile index overflows 15 bits")
     lcsr = ((local << 1) | slot_side).astype(np.uint16)
 
+    cptr64 = geom.cell_edge_ptr.astype(np.int64)
+    first_slot = cptr64[np.minimum(np.arange(n_blk + 1) * bc, n)]
+    seg = np.diff(first_slot)
+    seg_pad = (seg + 7) // 8 * 8
+    lptr = np.zeros(n_blk + 1, dtype=np.int64)
+    np.cumsum(seg_pad, out=lptr[1:])
+    lcsr_blk = np.zeros(int(lptr[-1]) + 8, dtype=np.uint16)
+    dest = lptr[slot_block] + (np.arange(slot_cell.size) - first_slot[slot_block])
+    lcsr_blk[dest] = lcsr
+    cptr_pad = np.full(n_blk * bc + 4, cptr64[-1], dtype=np.int64)
+    cptr_pad[: n + 1] = cptr64
+
     rptr, ridx = block_two_ring(*block_adjacency(ecl.astype(np.int32), ecr.astype(np.int32), n, bc))
     return TileLayout(
         n_cells=n,
@@ -135,14 +154,17 @@ def build_tile_layout(geom: MeshGeometry) -> TileLayout:
         tile_len=gather(geom.edge_len[order], 0.0, np.float32),
         tile_dzl=gather(geom.edge_dzL[order], 0.0, np.float32),
         tile_dzr=gather(geom.edge_dzR[order], 0.0, np.float32),
-        tile_ptr=ptr[:-1].astype(np.uint32),
+        tile_ptr=ptr.astype(np.uint32),
         tile_count=count.astype(np.uint32),
         tile_edge=rec,
-        cptr=geom.cell_edge_ptr.astype(np.uint32),
+        cptr=cptr_pad.astype(np.uint32),
         lcsr=lcsr,
+        lcsr_blk=lcsr_blk,
+        lcsr_ptr=lptr.astype(np.uint32),
+        max_block_slots=int(seg_pad.max()),
         ring_ptr=rptr.astype(np.uint32),
         ring_idx=ridx.astype(np.uint32) if ridx.size else np.zeros(1, np.uint32),
-        area=geom.area.astype(np.float32),
+        area=np.concatenate([geom.area.astype(np.float32), np.ones(n_blk * bc - n, np.float32)]),
     )
 
 

@@ -26,7 +26,7 @@ STATUS_MESSAGES = {
 _SIGNATURES: dict[str, tuple[list, object]] = {
     "swe_workspace_bytes": ([_U32], ctypes.c_size_t),
     "swe_tile_smem_bytes": ([_U32], ctypes.c_size_t),
-    "swe_blocks_per_sm": ([_U32, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "swe_configure": ([_P, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "swe_stage": ([_P, _P, _P, ctypes.c_int, _P], ctypes.c_int),
     "swe_apply_sources": ([_P, _P, _P, _P, _P], ctypes.c_int),
     "swe_block_dilate_compact": ([_P, _P, _P, ctypes.c_int, ctypes.c_int, _P], ctypes.c_int),
@@ -49,10 +49,10 @@ class SweMesh(ctypes.Structure):
         ("n_cells", _U32),
         ("n_blocks", _U32),
         ("max_tile_edges", _U32),
-        ("pad0", _U32),
+        ("max_block_slots", _U32),
         *[(name, _P) for name in (
             "tile_cl", "tile_cr", "tile_nx", "tile_ny", "tile_len", "tile_dzl", "tile_dzr", "tile_ptr",
-            "tile_count", "cptr", "lcsr", "area", "n_mann", "ring_ptr", "ring_idx",
+            "tile_count", "cptr", "lcsr", "area", "n_mann", "ring_ptr", "ring_idx", "lcsr_blk", "lcsr_ptr",
         )],
     ]
 
@@ -76,7 +76,7 @@ class SweParams(ctypes.Structure):
         ("track_clamp", _U32),
         ("active_set", _U32),
         ("grid", _U32),
-        ("pad", _U32),
+        ("kernel", _U32),
     ]
 
 

@@ -63,10 +63,11 @@ def test_status_strings_and_argument_checks(lib: ctypes.CDLL) -> None:
     assert lib.swe_volume_fp64(None, None, None, 0, None, None, None) == 1
     assert lib.swe_workspace_bytes(1_000_000) > 3907 * 4
     assert lib.swe_tile_smem_bytes(900) >= 900 * 24
+    assert lib.swe_configure(None, 0, None) == 1
 
 
 def test_ctypes_structs_match_the_header_layout() -> None:
-    assert ctypes.sizeof(native.SweMesh) == 16 + 15 * 8
+    assert ctypes.sizeof(native.SweMesh) == 16 + 17 * 8
     assert ctypes.sizeof(native.SweState) == 14 * 8
     assert ctypes.sizeof(native.SweParams) == 32
     assert ctypes.sizeof(native.SweSources) == 24

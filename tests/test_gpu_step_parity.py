@@ -76,11 +76,17 @@ CASES: dict[str, Callable] = {
 }
 
 
-def make_solver(grid, s: fp64_step.State):
+def make_solver(grid, s: fp64_step.State, kernel: str = "staged", grid_limit: int | None = None):
     from inundation_b200.backend import SWESolverB200Resident
 
     f32 = [a.astype(np.float32) for a in (s.h, s.hu, s.hv)]
-    return SWESolverB200Resident(grid, None, *f32, np.full(grid.N, MANNING, np.float32), dry_tol=DRY_TOL)
+    solver = SWESolverB200Resident(grid, None, *f32, np.full(grid.N, MANNING, np.float32), dry_tol=DRY_TOL)
+    solver.stage_kernel = kernel
+    if grid_limit is not None:
+        # Few persistent CTAs: each loops over many blocks, so the staged kernel's
+        # prefetch of the next block overlaps the current one.
+        solver._grids = {k: min(v, grid_limit) for k, v in solver._grids.items()}
+    return solver
 
 
 def make_oracle(grid, s: fp64_step.State) -> ResidentOracle:
@@ -106,15 +112,17 @@ def assert_same_bits(a: np.ndarray, b: np.ndarray, what: str) -> None:
     assert bad.size == 0, f"{what}: {bad.size} cells differ from the FP32 oracle (first {bad[:5].tolist()})"
 
 
+@pytest.mark.parametrize("kernel,grid_limit", [("staged", None), ("plain", None), ("staged", 5)],
+                         ids=["staged", "plain", "staged-5ctas"])
 @pytest.mark.parametrize("case", list(CASES))
-def test_steps_match_fp64_and_fp32_oracles(case: str, grid) -> None:
+def test_steps_match_fp64_and_fp32_oracles(case: str, kernel: str, grid_limit, grid) -> None:
     s0 = CASES[case](grid)
     n = np.full(grid.N, MANNING, np.float32)
     want = fp64_step.run_steps(
         grid, s0.h.astype(np.float32), s0.hu.astype(np.float32), s0.hv.astype(np.float32), n, DT, STEPS,
         g=GRAVITY_G, dry_tol=DRY_TOL,
     )
-    solver = make_solver(grid, s0)
+    solver = make_solver(grid, s0, kernel, grid_limit)
     got = step(solver, STEPS)
     assert_close(got, want, ATOL_H, ATOL_Q)
     oracle = make_oracle(grid, s0)
