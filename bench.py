@@ -54,13 +54,13 @@ def parse_args() -> argparse.Namespace:
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=["dam_break", "full_wet"], default="dam_break")
+    ap.add_argument("--workload", choices=["dam_break", "full_wet", "one_cell"], default="dam_break")
     ap.add_argument("--cells", type=int, default=1_000_000)
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--chunk", type=int, default=500, help="steps per captured graph in the timed region")
-    ap.add_argument("--kernel", choices=["staged", "plain"], default="staged", help="stage kernel variant")
+    ap.add_argument("--kernel", choices=["tiled", "plain"], default="tiled", help="stage kernel variant")
     return ap.parse_args()
 
 
@@ -78,6 +78,12 @@ def build_scenario(name: str, cells: int, seed: int):
         sc.h0 = h
         sc.hu0 = (0.2 * np.sin(2 * np.pi * x / side) * h).astype(np.float32)
         sc.name = "full_wet"
+    elif name == "one_cell":
+        # A single wet cell: the launch latency of a step with a handful of active blocks.
+        h = np.zeros(sc.geom.N, np.float32)
+        h[sc.geom.N // 2] = 1.0
+        sc.h0 = h
+        sc.name = "one_cell"
     return sc
 
 

@@ -10,6 +10,10 @@
  * The entry points replace the device dispatches the reference records in
  * inundation/vulkan/gpu_resident_batch.py. Each declaration names the
  * reference kernel(s) or host call it stands for (file:line).
+ *
+ * A mesh may hold several independent meshes ("instances", a batch): each
+ * starts on a 256-cell block boundary and has its own clock, dt and CFL bound.
+ * A single mesh is a batch of one.
  */
 #ifndef INUNDATION_B200_H
 #define INUNDATION_B200_H
@@ -32,8 +36,8 @@ enum swe_status {
     SWE_ERR_MATH = 4,         /* the device arithmetic lost the two-sum error term */
 };
 
-/* Control block of the integer clock: 48 bytes, the layout of the reference's
-   RESIDENT_CTRL_DTYPE (inundation/vulkan/gpu_resident_batch.py:64-77). */
+/* Control block of one instance's integer clock: 48 bytes, the layout of the
+   reference's RESIDENT_CTRL_DTYPE (inundation/vulkan/gpu_resident_batch.py:64-77). */
 typedef struct {
     uint64_t now_ticks;
     uint64_t stop_ticks;
@@ -46,24 +50,26 @@ typedef struct {
     uint32_t error;  /* set by the device: 1 = a bounded wait for staged data timed out */
 } swe_ctrl_t;
 
-/* Static mesh in the block-tile layout (device pointers).
-   Block b = cells [256 b, 256 b + 256). Its tile is the contiguous range
-   [tile_ptr[b], tile_ptr[b + 1]) of the tile_* arrays, tile_count[b] records
-   and then padding to a multiple of 32: first the edges whose left cell is
-   in b (the reference's resident edge order, gpu_resident_batch.py:175), then
-   the edges whose right cell is in b and left cell is not.
+/* Static mesh in two tile layouts (device pointers).
+   Block b = cells [256 b, 256 b + 256), of which block_cells[b] are real (the
+   rest pad an instance to whole blocks). Its 256-cell tile is the contiguous
+   range [tile_ptr[b], tile_ptr[b + 1]) of the tile_* arrays, tile_count[b]
+   records then padding to a multiple of 32: first the edges whose left cell
+   is in b (the reference's resident edge order, gpu_resident_batch.py:175),
+   then the edges whose right cell is in b and left cell is not.
    lcsr[k] = (position in the tile << 1) | is_right for the CSR slots k of each
    cell, in the reference's per-cell order (inundation/mesh/geometry.py:454-468,
-   remapped as blocks.py:33-44); lcsr_blk holds the same entries regrouped per
-   block, block b's from lcsr_blk[lcsr_ptr[b]] (a multiple of 8).
-   Every per-cell array (area, n_mann and all state arrays) holds
-   n_blocks * 256 entries; cptr holds n_blocks * 256 + 4, repeating the total
-   past n_cells. These paddings let whole blocks be bulk-copied. */
+   remapped as blocks.py:33-44).
+   The 64-cell compute tiles (tile t = cells [64 t, 64 t + 64), four per block)
+   are laid out the same way in the sub_* arrays, with their local CSR regrouped
+   per tile from sub_lcsr[sub_lcsr_ptr[t]] (multiples of 8).
+   Every per-cell array (area, n_mann and all state arrays) holds n_blocks * 256
+   entries; cptr holds n_blocks * 256 + 4, flat across the batch. */
 typedef struct {
-    uint32_t n_cells;
+    uint32_t n_cells;         /* cells, padding between instances included */
     uint32_t n_blocks;
     uint32_t max_tile_edges;  /* the largest tile_count */
-    uint32_t max_block_slots; /* the largest lcsr_ptr[b + 1] - lcsr_ptr[b] */
+    uint32_t n_inst;          /* instances in the batch */
     const int32_t *tile_cl;   /* left cell */
     const int32_t *tile_cr;   /* right cell, -1 on a wall */
     const float *tile_nx;
@@ -74,26 +80,41 @@ typedef struct {
     const uint32_t *tile_ptr;   /* n_blocks + 1 */
     const uint32_t *tile_count; /* n_blocks */
     const uint32_t *cptr;       /* n_blocks * 256 + 4 */
-    const uint16_t *lcsr;       /* cptr[n_cells] */
+    const uint16_t *lcsr;       /* one per CSR slot */
     const float *area;
     const float *n_mann;
     const uint32_t *ring_ptr;   /* block two-ring CSR (blocks.py:93-118) */
     const uint32_t *ring_idx;
-    const uint16_t *lcsr_blk;
-    const uint32_t *lcsr_ptr;   /* n_blocks + 1 */
+    const uint32_t *block_inst;  /* n_blocks: instance of each block */
+    const uint32_t *block_cells; /* n_blocks: real cells of each block */
+    uint32_t max_sub_edges;
+    uint32_t max_sub_slots;
+    const int32_t *sub_cl;
+    const int32_t *sub_cr;
+    const float *sub_nx;
+    const float *sub_ny;
+    const float *sub_len;
+    const float *sub_dzl;
+    const float *sub_dzr;
+    const uint32_t *sub_ptr;      /* n_blocks * 4 + 1 */
+    const uint32_t *sub_count;    /* n_blocks * 4 */
+    const uint16_t *sub_lcsr;
+    const uint32_t *sub_lcsr_ptr; /* n_blocks * 4 + 1 */
 } swe_mesh_t;
 
-/* Mutable state and the per-run workspace (device pointers). */
+/* Mutable state and the run workspace (device pointers). */
 typedef struct {
     float *h, *hu, *hv, *h_lo;     /* committed state; h_lo: compensated low word */
     float *h1, *hu1, *hv1, *h1_lo; /* Heun predictor */
     float *clamp_mass;             /* per-cell positivity-clamp volume (diagnostic) */
     uint32_t *blk;                 /* 3 words per block: wet, active, forced */
     uint32_t *active_list;         /* n_blocks: active blocks of the current step */
-    uint32_t *sched;               /* 8 words: [0] active count, [1] next count, [2] done CTAs, [3] cells of the
-                                      active blocks, [4] next cells, [6..7] uint64 cells computed over real steps */
-    uint32_t *dt_buf;              /* [0] this step's dt (float bits, 0 = no-op), [1] next CFL bound */
-    swe_ctrl_t *ctrl;
+    uint32_t *items;               /* 4 words per 64-cell tile: the tiled kernel's work items */
+    uint32_t *sched;               /* 16 words: [0] active blocks, [1] next blocks, [2] done CTAs, [3] work items,
+                                      [4] next items, [6..7] uint64 cells computed over real steps, others zero */
+    uint32_t *dt_buf;              /* 4 words per instance: [0] this step's dt (float bits, 0 = no-op),
+                                      [1] the next step's CFL bound */
+    swe_ctrl_t *ctrl;              /* one per instance */
 } swe_state_t;
 
 typedef struct {
@@ -103,33 +124,41 @@ typedef struct {
     uint32_t compensated; /* depth as a (h, h_lo) two-sum pair */
     uint32_t track_clamp; /* accumulate the clamp diagnostic */
     uint32_t active_set;  /* skip blocks outside the two-ring of wet blocks */
-    uint32_t grid;        /* CTAs of the persistent per-block kernels (0 = one per block) */
-    uint32_t kernel;      /* stage kernel: 0 = bulk-copy staged tiles (default), 1 = plain loads */
+    uint32_t grid;        /* CTAs of the persistent stage kernels (0 = a default) */
+    uint32_t kernel;      /* stage kernel: 0 = 64-cell tiles staged by bulk copies (default),
+                             1 = 256-cell blocks with plain loads */
 } swe_params_t;
 
-/* Sparse sources: n pairs (cell, dh/dt) on the device. */
+/* Sparse sources (device pointers): source k adds dt * rate[k] to cell
+   cells[k], times the value of hydrograph hydro[k] at its instance's clock
+   when hydro[k] != 0xFFFFFFFF. Hydrograph j is piecewise linear through the
+   knots (knot_t[i], knot_q[i]), i in [knot_ptr[j], knot_ptr[j + 1]), constant
+   outside them. */
 typedef struct {
     const uint32_t *cells;
     const float *rate;
+    const uint32_t *hydro;
+    const uint32_t *knot_ptr;
+    const float *knot_t;
+    const float *knot_q;
     uint32_t count;
-    uint32_t pad;
+    uint32_t n_hydro;
 } swe_sources_t;
 
-/* Bytes of device workspace: active list + sched words + dt words (+ volume partials). */
-size_t swe_workspace_bytes(uint32_t n_cells);
-
-/* Dynamic shared memory one per-block CTA needs for a tile of max_tile_edges. */
-size_t swe_tile_smem_bytes(uint32_t max_tile_edges);
+/* Bytes of device workspace of a mesh of n_blocks blocks and n_inst
+   instances: active list, work items, sched words, dt words and control
+   blocks. */
+size_t swe_workspace_bytes(uint32_t n_blocks, uint32_t n_inst);
 
 /* Sets the shared-memory size of every per-block kernel for this mesh (call
    once, before any stream capture) and returns the persistent CTAs per SM of
-   the chosen stage kernel (0 staged, 1 plain). */
+   the chosen stage kernel (swe_params_t.kernel). */
 int swe_configure(const swe_mesh_t *mesh, int kernel, int *blocks_per_sm);
 
-/* One Heun stage over the active blocks, fused: edge fluxes of each block's
-   tile into shared memory, the fixed-order per-cell gather and the update.
-   stage 0 = predictor, 1 = corrector (adds the next step's CFL bound and the
-   wet marks). Replaces flux_resident_gather + update_resident_gather[_comp]
+/* One Heun stage over the active blocks, fused: edge fluxes of each tile into
+   shared memory, the fixed-order per-cell gather and the update. stage 0 =
+   predictor, 1 = corrector (adds the next step's CFL bound and the wet marks).
+   Replaces flux_resident_gather + update_resident_gather[_comp]
    (inundation/vulkan/shaders/resident.py:187-291 and 401-513). */
 int swe_stage(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params_t *params, int stage,
               swe_stream_t stream);
@@ -141,8 +170,9 @@ int swe_apply_sources(const swe_mesh_t *mesh, const swe_state_t *state, const sw
                       const swe_sources_t *sources, swe_stream_t stream);
 
 /* Active flags = (wet | forced) dilated over each block's two-ring, compacted
-   into active_list; then, when control_mode >= 0, step_control in the last
-   CTA. force = 1 also on a no-op step. Replaces block_dilate + step_control
+   into active_list and the tile work items; then, when control_mode >= 0,
+   step_control of every instance in the last CTA. An instance on a no-op step
+   keeps its flags unless force = 1. Replaces block_dilate + step_control
    (resident.py:778-805, 813-885). */
 int swe_block_dilate_compact(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params_t *params,
                              int force, int control_mode, swe_stream_t stream);
@@ -152,15 +182,15 @@ int swe_block_dilate_compact(const swe_mesh_t *mesh, const swe_state_t *state, c
 int swe_block_mark(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params_t *params,
                    swe_stream_t stream);
 
-/* Prologue CFL bound of the current state into dt_buf[0] (reset to 1e30
-   first). Replaces dt_reset + cfl_edge_gather + cfl_gather
+/* Prologue CFL bound of the current state into each instance's dt word 0
+   (reset to 1e30 first). Replaces dt_reset + cfl_edge_gather + cfl_gather
    (cfl.py:130-166, resident.py:528-610). */
 int swe_cfl_prologue(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params_t *params,
                      swe_stream_t stream);
 
-/* Integer-tick step control; mode 0 START, 1 STEP, 2 RETARGET.
-   Replaces step_control (resident.py:813-885). */
-int swe_step_control(swe_ctrl_t *ctrl, uint32_t *dt_buf, int mode, swe_stream_t stream);
+/* Integer-tick step control of n_inst instances; mode 0 START, 1 STEP,
+   2 RETARGET. Replaces step_control (resident.py:813-885). */
+int swe_step_control(swe_ctrl_t *ctrl, uint32_t *dt_buf, uint32_t n_inst, int mode, swe_stream_t stream);
 
 /* Whole prologue: block_mark, forced dilation, CFL bound, START
    (gpu_resident_batch.py:567-591). */

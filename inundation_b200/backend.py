@@ -78,8 +78,9 @@ class SWESolverB200Resident:
     deterministic: bool = True
     compensated: bool = True
     cfl_safety: float = 1.0
-    # Stage kernel: "staged" (bulk-copied tiles, double-buffered) or "plain" (direct loads).
-    stage_kernel: str = "staged"
+    # Stage kernel: "tiled" (64-cell tiles from the dilation's work items, staged by bulk copies)
+    # or "plain" (256-cell blocks, direct loads).
+    stage_kernel: str = "tiled"
 
     def __init__(
         self,
@@ -143,31 +144,28 @@ class SWESolverB200Resident:
         return torch.from_numpy(np.ascontiguousarray(a)).to(self.device)
 
     def _upload_mesh(self, L: TileLayout, n0: NDArray[np.float32]) -> None:
-        t = {
-            "tile_cl": self._dev(L.tile_cl),
-            "tile_cr": self._dev(L.tile_cr),
-            "tile_nx": self._dev(L.tile_nx),
-            "tile_ny": self._dev(L.tile_ny),
-            "tile_len": self._dev(L.tile_len),
-            "tile_dzl": self._dev(L.tile_dzl),
-            "tile_dzr": self._dev(L.tile_dzr),
-            "tile_ptr": self._dev(_i32(L.tile_ptr)),
-            "tile_count": self._dev(_i32(L.tile_count)),
-            "cptr": self._dev(_i32(L.cptr)),
-            "lcsr": self._dev(L.lcsr.view(np.int16)),
-            "area": self._dev(L.area),
-            "n_mann": self._dev(np.concatenate([n0, np.full(L.n_padded_cells - L.n_cells, 0.03, np.float32)])),
-            "ring_ptr": self._dev(_i32(L.ring_ptr)),
-            "ring_idx": self._dev(_i32(L.ring_idx)),
-            "lcsr_blk": self._dev(L.lcsr_blk.view(np.int16)),
-            "lcsr_ptr": self._dev(_i32(L.lcsr_ptr)),
-        }
+        B, S = L.blocks, L.subs
+        t = {"cptr": self._dev(_i32(L.cptr)), "area": self._dev(L.area),
+             "n_mann": self._dev(np.concatenate([n0, np.full(L.n_padded_cells - L.n_cells, 0.03, np.float32)])),
+             "ring_ptr": self._dev(_i32(L.ring_ptr)), "ring_idx": self._dev(_i32(L.ring_idx))}
+        for prefix, T in (("tile_", B), ("sub_", S)):
+            for name in ("cl", "cr", "nx", "ny", "len", "dzl", "dzr"):
+                t[prefix + name] = self._dev(getattr(T, name))
+            t[prefix + "ptr"] = self._dev(_i32(T.ptr))
+            t[prefix + "count"] = self._dev(_i32(T.count))
+        t["lcsr"] = self._dev(B.lcsr.view(np.int16))
+        t["block_inst"] = self._dev(np.zeros(L.n_blocks, np.int32))
+        t["block_cells"] = self._dev(_i32(L.block_cells))
+        t["sub_lcsr"] = self._dev(S.lcsr_blk.view(np.int16))
+        t["sub_lcsr_ptr"] = self._dev(_i32(S.lcsr_ptr))
         self._mesh_t = t
         m = native.SweMesh()
         m.n_cells = L.n_cells
         m.n_blocks = L.n_blocks
-        m.max_tile_edges = L.max_tile_edges
-        m.max_block_slots = L.max_block_slots
+        m.max_tile_edges = B.max_edges
+        m.n_inst = 1
+        m.max_sub_edges = S.max_edges
+        m.max_sub_slots = S.max_slots
         for name, tensor in t.items():
             setattr(m, name, tensor.data_ptr())
         self._mesh = m
@@ -177,13 +175,16 @@ class SWESolverB200Resident:
             per_sm = ctypes.c_int(0)
             with torch.cuda.device(self.device):
                 native.check(self._lib.swe_configure(ctypes.byref(m), kernel, ctypes.byref(per_sm)), "swe_configure")
-            self._grids[kernel] = max(1, min(L.n_blocks, per_sm.value * self._sms))
+            units = 4 * L.n_blocks if kernel == 0 else L.n_blocks  # the tiled kernel works on 64-cell tiles
+            self._grids[kernel] = max(1, min(units, per_sm.value * self._sms))
+
+    _KERNELS = {"tiled": 0, "plain": 1}
 
     @property
     def _kernel(self) -> int:
-        if self.stage_kernel not in ("staged", "plain"):
-            raise ValueError(f"stage_kernel must be 'staged' or 'plain', got {self.stage_kernel!r}")
-        return 0 if self.stage_kernel == "staged" else 1
+        if self.stage_kernel not in self._KERNELS:
+            raise ValueError(f"stage_kernel must be one of {sorted(self._KERNELS)}, got {self.stage_kernel!r}")
+        return self._KERNELS[self.stage_kernel]
 
     def _alloc_state(self) -> None:
         n, nb, dev = self.layout.n_padded_cells, self.n_blocks, self.device
@@ -191,7 +192,8 @@ class SWESolverB200Resident:
         self._t = {name: z() for name in ("h", "hu", "hv", "h_lo", "h1", "hu1", "hv1", "h1_lo", "clamp_mass")}
         self._blk = torch.zeros(3 * nb, dtype=torch.int32, device=dev)
         self._active_list = torch.zeros(nb, dtype=torch.int32, device=dev)
-        self._sched = torch.zeros(4, dtype=torch.int64, device=dev)  # 8 uint32 words
+        self._items = torch.zeros(16 * nb, dtype=torch.int32, device=dev)  # 4 tiles x 4 words per block
+        self._sched = torch.zeros(8, dtype=torch.int64, device=dev)  # 16 uint32 words
         self._dt_buf = torch.tensor([0, _SENTINEL_BITS, 0, 0], dtype=torch.int64, device=dev).to(torch.int32)
         self._ctrl_dev = torch.zeros(6, dtype=torch.int64, device=dev)
         self._ctrl_pinned = torch.zeros(6, dtype=torch.int64).pin_memory()
@@ -203,6 +205,7 @@ class SWESolverB200Resident:
             setattr(s, name, tensor.data_ptr())
         s.blk = self._blk.data_ptr()
         s.active_list = self._active_list.data_ptr()
+        s.items = self._items.data_ptr()
         s.sched = self._sched.data_ptr()
         s.dt_buf = self._dt_buf.data_ptr()
         s.ctrl = self._ctrl_dev.data_ptr()
@@ -350,7 +353,8 @@ class SWESolverB200Resident:
     def _enqueue_prologue(self) -> None:
         p = self._params()
         with torch.cuda.stream(self._stream):
-            self._sched[:3].zero_()  # counters; words 6-7 keep the computed-cells total
+            self._sched[:3].zero_()  # list counters; words 6-7 keep the computed-cells total
+            self._sched[4:].zero_()
             native.check(
                 self._lib.swe_prologue(
                     ctypes.byref(self._mesh), ctypes.byref(self._state), ctypes.byref(p), self._cuda_stream
@@ -358,11 +362,21 @@ class SWESolverB200Resident:
                 "swe_prologue",
             )
 
-    def _enqueue_step_control(self, mode: int) -> None:
+    def _enqueue_retarget(self) -> None:
+        """RETARGET the clock to a new stop, rebuilding the active lists first.
+
+        A no-op step leaves its instance out of the lists, so the lists are
+        rebuilt by a forced dilation (the flags come out the same: they were
+        dilated from the same wet marks after the last real step).
+        """
+        p = self._params()
         with torch.cuda.stream(self._stream):
             native.check(
-                self._lib.swe_step_control(self._ctrl_dev.data_ptr(), self._dt_buf.data_ptr(), mode, self._cuda_stream),
-                "swe_step_control",
+                self._lib.swe_block_dilate_compact(
+                    ctypes.byref(self._mesh), ctypes.byref(self._state), ctypes.byref(p), 1, RETARGET,
+                    self._cuda_stream,
+                ),
+                "swe_block_dilate_compact",
             )
 
     def _enqueue_steps(self, n_steps: int, params: native.SweParams, sources: native.SweSources) -> None:
@@ -467,7 +481,7 @@ class SWESolverB200Resident:
             ctrl["stop_ticks"] = stop
             self._sync_ctrl_to_device()
             if planned:
-                self._enqueue_step_control(RETARGET)
+                self._enqueue_retarget()
             else:
                 self._enqueue_prologue()
                 planned = True

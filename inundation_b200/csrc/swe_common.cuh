@@ -1,0 +1,187 @@
+// Shared device and host helpers of the shallow-water kernels.
+//
+// Meshes: cells in Hilbert order, grouped in 256-cell blocks (the active-set
+// unit of the reference, inundation/tuning.py:53-55) and 64-cell compute
+// tiles (four per block). A batch concatenates several meshes (instances),
+// each starting on a block boundary; block_inst names a block's instance,
+// block_cells its real cells. Every instance has its own clock (control
+// block) and its own dt words: dt_buf[4 i] is the dt of its current step
+// (0 = no-op), dt_buf[4 i + 1] the CFL bound reduced for its next step.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/inundation_b200.h"
+#include "swe_math.cuh"
+
+namespace swe {
+
+constexpr int kBlockCells = 256;
+constexpr int kThreads = 256;
+constexpr int kTileCells = 64;
+constexpr int kTileThreads = 128;
+constexpr uint32_t kBlkWords = 3, kBlkWet = 0, kBlkActive = 1, kBlkForced = 2;
+constexpr uint32_t kNoBound = 0xFFFFFFFFu;
+constexpr uint32_t kDtWords = 4;
+constexpr uint64_t kWaitLimitNs = 2000000000ull;  // bound of every device wait: 2 s
+
+// sched words
+constexpr int kSchedActive = 0;     // blocks in active_list for the current step
+constexpr int kSchedNext = 1;       // blocks appended by the dilation
+constexpr int kSchedDone = 2;       // CTAs of the dilation that finished
+constexpr int kSchedItems = 3;      // tile work items of the current step
+constexpr int kSchedNextItems = 4;  // tile work items appended by the dilation
+constexpr int kSchedComputed = 6;   // [6,7]: uint64 cells computed over real steps
+
+// A tile work item: x = tile | (real cells << 25), y = first edge record,
+// z = first local-CSR entry, w = edge count | (padded slot count << 11) | (instance << 22).
+__device__ __forceinline__ uint4 make_item(uint32_t tile, uint32_t cells, uint32_t e0, uint32_t l0, uint32_t ne,
+                                           uint32_t lp, uint32_t inst) {
+    return make_uint4(tile | (cells << 25), e0, l0, ne | (lp << 11) | (inst << 22));
+}
+
+__device__ __forceinline__ bool block_active(const uint32_t *blk, uint32_t b) {
+    return blk[kBlkWords * b + kBlkActive] != 0u;
+}
+
+// The stage's input state of cell c: the predictor in the corrector, except
+// in an inactive block, whose predictor is stale (resident.py:209-226). In
+// the corrector both candidates are loaded with the flag, in one round trip.
+template <int STAGE>
+__device__ __forceinline__ void load_state(const swe_state_t &s, int c, float &h, float &hu, float &hv) {
+    if (STAGE == 0) {
+        h = s.h[c];
+        hu = s.hu[c];
+        hv = s.hv[c];
+    } else {
+        const bool pred = block_active(s.blk, static_cast<uint32_t>(c) >> 8);
+        const float a0 = s.h1[c], a1 = s.hu1[c], a2 = s.hv1[c];
+        const float b0 = s.h[c], b1 = s.hu[c], b2 = s.hv[c];
+        h = pred ? a0 : b0;
+        hu = pred ? a1 : b1;
+        hv = pred ? a2 : b2;
+    }
+}
+
+__device__ __forceinline__ uint32_t block_min_any(uint32_t v, uint32_t *scratch) {
+    v = __reduce_min_sync(0xFFFFFFFFu, v);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    if (lane == 0) scratch[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = (lane < nw) ? scratch[lane] : kNoBound;
+        w = __reduce_min_sync(0xFFFFFFFFu, w);
+        if (lane == 0) scratch[0] = w;
+    }
+    __syncthreads();
+    const uint32_t r = scratch[0];
+    __syncthreads();
+    return r;
+}
+
+// -- bulk copies (TMA, 1-D, no multicast) into shared memory on an mbarrier --------------------
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_barrier_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return done != 0u;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// True once the barrier's phase of this parity completed; false after the deadline.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    if (mbar_test(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    while (!mbar_test(bar, parity)) {
+        if (global_ns() - t0 > kWaitLimitNs) return false;
+    }
+    return true;
+}
+
+// -- integer-tick step control (resident.py:813-885) ---------------------------------------------
+__device__ __forceinline__ void step_control(swe_ctrl_t *c, uint32_t *dt_buf, int mode) {
+    float raw;
+    if (mode == 0) {
+        raw = __uint_as_float(dt_buf[0]);
+        c->last_raw = raw;
+    } else if (mode == 1) {
+        const uint32_t done = c->dt_ticks;
+        c->now_ticks += static_cast<uint64_t>(done);
+        if (done > 0u) {
+            c->steps += 1u;
+            raw = __uint_as_float(dt_buf[1]);
+            c->last_raw = raw;
+        } else {
+            raw = c->last_raw;  // a no-op step computed no bound
+        }
+    } else {
+        raw = c->last_raw;
+    }
+    const uint64_t remaining = (c->stop_ticks > c->now_ticks) ? c->stop_ticks - c->now_ticks : 0ull;
+    uint32_t ticks;
+    if (remaining == 0ull || raw < 1e-10f || raw != raw) {
+        ticks = 0u;  // window done, or a degenerate bound: the host sees no progress
+    } else if (raw >= 1e10f) {
+        ticks = c->dry_dt_ticks;  // no wet edge anywhere
+    } else {
+        const float cap = static_cast<float>(c->dt_max_ticks) / kTicksPerSecond;
+        ticks = static_cast<uint32_t>(gmin(raw * c->cfl_safety, cap) * kTicksPerSecond);
+    }
+    if (c->dt_max_ticks < ticks) ticks = c->dt_max_ticks;
+    if (static_cast<uint64_t>(ticks) > remaining) ticks = static_cast<uint32_t>(remaining);
+    c->dt_ticks = ticks;
+    dt_buf[0] = __float_as_uint(static_cast<float>(ticks) / kTicksPerSecond);
+    dt_buf[1] = __float_as_uint(kDtSentinel);
+}
+
+// -- host helpers --------------------------------------------------------------------------------
+inline int check_launch() { return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ERR_CUDA; }
+
+template <typename K>
+inline int set_smem(K kernel, size_t bytes) {
+    if (bytes > 227 * 1024) return SWE_ERR_TOO_LARGE;
+    if (bytes > 48 * 1024 &&
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)) != cudaSuccess)
+        return SWE_ERR_CUDA;
+    return SWE_OK;
+}
+
+inline bool mesh_ok(const swe_mesh_t *m) {
+    return m && m->n_cells && m->n_blocks && m->n_inst && m->tile_cl && m->tile_cr && m->tile_nx && m->tile_ny &&
+           m->tile_len && m->tile_dzl && m->tile_dzr && m->tile_ptr && m->tile_count && m->cptr && m->lcsr &&
+           m->area && m->n_mann && m->ring_ptr && m->ring_idx && m->sub_cl && m->sub_cr && m->sub_nx && m->sub_ny &&
+           m->sub_len && m->sub_dzl && m->sub_dzr && m->sub_ptr && m->sub_count && m->sub_lcsr && m->sub_lcsr_ptr &&
+           m->block_inst && m->block_cells;
+}
+
+inline bool state_ok(const swe_state_t *s) {
+    return s && s->h && s->hu && s->hv && s->h_lo && s->h1 && s->hu1 && s->hv1 && s->h1_lo && s->clamp_mass &&
+           s->blk && s->active_list && s->items && s->sched && s->dt_buf && s->ctrl;
+}
+
+}  // namespace swe

@@ -97,7 +97,7 @@ __device__ __forceinline__ void hllc(const Phys &p, float hL, float hqnL, float 
     const float unL = safe_vel(p, hL, hqnL), utL = safe_vel(p, hL, hqtL);
     const float unR = safe_vel(p, hR, hqnR), utR = safe_vel(p, hR, hqtR);
     float SL, SR;
-    hllc_speeds(p, hL, unL, hR, unR, SL, SR);
+    hllc_speeds_fast(p, hL, unL, hR, unR, SL, SR);
     smax = gmax(fabsf(SL), fabsf(SR));
     const float num_sm = SL * hR * (unR - SR) - SR * hL * (unL - SL);
     const float den_sm = hR * (unR - SR) - hL * (unL - SL);

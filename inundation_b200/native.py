@@ -17,22 +17,21 @@ _U32 = ctypes.c_uint32
 STATUS_MESSAGES = {
     1: "invalid argument",
     2: "CUDA launch or runtime error",
-    3: "size beyond a fixed limit (an edge tile larger than shared memory, or more cells than the "
-    "allocation-free volume's static scratch holds)",
+    3: "size beyond a fixed limit (an edge tile larger than shared memory or than a work item's fields, "
+    "or more cells than the allocation-free volume's static scratch holds)",
     4: "device arithmetic lost the two-sum error term",
 }
 
 # Every function the header declares, with its argument and result types.
 _SIGNATURES: dict[str, tuple[list, object]] = {
-    "swe_workspace_bytes": ([_U32], ctypes.c_size_t),
-    "swe_tile_smem_bytes": ([_U32], ctypes.c_size_t),
+    "swe_workspace_bytes": ([_U32, _U32], ctypes.c_size_t),
     "swe_configure": ([_P, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "swe_stage": ([_P, _P, _P, ctypes.c_int, _P], ctypes.c_int),
     "swe_apply_sources": ([_P, _P, _P, _P, _P], ctypes.c_int),
     "swe_block_dilate_compact": ([_P, _P, _P, ctypes.c_int, ctypes.c_int, _P], ctypes.c_int),
     "swe_block_mark": ([_P, _P, _P, _P], ctypes.c_int),
     "swe_cfl_prologue": ([_P, _P, _P, _P], ctypes.c_int),
-    "swe_step_control": ([_P, _P, ctypes.c_int, _P], ctypes.c_int),
+    "swe_step_control": ([_P, _P, _U32, ctypes.c_int, _P], ctypes.c_int),
     "swe_prologue": ([_P, _P, _P, _P], ctypes.c_int),
     "swe_step": ([_P, _P, _P, _P, _P], ctypes.c_int),
     "swe_volume_partials": ([_U32], _U32),
@@ -49,10 +48,16 @@ class SweMesh(ctypes.Structure):
         ("n_cells", _U32),
         ("n_blocks", _U32),
         ("max_tile_edges", _U32),
-        ("max_block_slots", _U32),
+        ("n_inst", _U32),
         *[(name, _P) for name in (
             "tile_cl", "tile_cr", "tile_nx", "tile_ny", "tile_len", "tile_dzl", "tile_dzr", "tile_ptr",
-            "tile_count", "cptr", "lcsr", "area", "n_mann", "ring_ptr", "ring_idx", "lcsr_blk", "lcsr_ptr",
+            "tile_count", "cptr", "lcsr", "area", "n_mann", "ring_ptr", "ring_idx", "block_inst", "block_cells",
+        )],
+        ("max_sub_edges", _U32),
+        ("max_sub_slots", _U32),
+        *[(name, _P) for name in (
+            "sub_cl", "sub_cr", "sub_nx", "sub_ny", "sub_len", "sub_dzl", "sub_dzr", "sub_ptr", "sub_count",
+            "sub_lcsr", "sub_lcsr_ptr",
         )],
     ]
 
@@ -61,8 +66,8 @@ class SweState(ctypes.Structure):
     _fields_ = [
         (name, _P)
         for name in (
-            "h", "hu", "hv", "h_lo", "h1", "hu1", "hv1", "h1_lo", "clamp_mass", "blk", "active_list", "sched",
-            "dt_buf", "ctrl",
+            "h", "hu", "hv", "h_lo", "h1", "hu1", "hv1", "h1_lo", "clamp_mass", "blk", "active_list", "items",
+            "sched", "dt_buf", "ctrl",
         )
     ]
 
@@ -81,7 +86,11 @@ class SweParams(ctypes.Structure):
 
 
 class SweSources(ctypes.Structure):
-    _fields_ = [("cells", _P), ("rate", _P), ("count", _U32), ("pad", _U32)]
+    _fields_ = [
+        *[(name, _P) for name in ("cells", "rate", "hydro", "knot_ptr", "knot_t", "knot_q")],
+        ("count", _U32),
+        ("n_hydro", _U32),
+    ]
 
 
 _LIB: ctypes.CDLL | None = None

@@ -59,18 +59,18 @@ def test_status_strings_and_argument_checks(lib: ctypes.CDLL) -> None:
     assert lib.swe_stage(None, None, None, 0, None) == 1
     assert lib.swe_step(None, None, None, None, None) == 1
     assert lib.swe_prologue(None, None, None, None) == 1
-    assert lib.swe_step_control(None, None, 0, None) == 1
+    assert lib.swe_step_control(None, None, 1, 0, None) == 1
     assert lib.swe_volume_fp64(None, None, None, 0, None, None, None) == 1
-    assert lib.swe_workspace_bytes(1_000_000) > 3907 * 4
-    assert lib.swe_tile_smem_bytes(900) >= 900 * 24
+    assert lib.swe_workspace_bytes(3907, 1) >= 3907 * 4 * 17 + 64 + 16 + 48
+    assert lib.swe_workspace_bytes(3907, 64) == lib.swe_workspace_bytes(3907, 1) + 63 * (16 + 48)
     assert lib.swe_configure(None, 0, None) == 1
 
 
 def test_ctypes_structs_match_the_header_layout() -> None:
-    assert ctypes.sizeof(native.SweMesh) == 16 + 17 * 8
-    assert ctypes.sizeof(native.SweState) == 14 * 8
+    assert ctypes.sizeof(native.SweMesh) == 16 + 17 * 8 + 8 + 11 * 8
+    assert ctypes.sizeof(native.SweState) == 15 * 8
     assert ctypes.sizeof(native.SweParams) == 32
-    assert ctypes.sizeof(native.SweSources) == 24
+    assert ctypes.sizeof(native.SweSources) == 6 * 8 + 8
 
 
 @pytest.mark.parametrize("name", ["voronoi", "valley", "mixed"])
@@ -79,19 +79,23 @@ def test_tile_layout_resolves_every_csr_slot(name: str) -> None:
     raw = build_geometry(GEO[f"{name}_in_verts"], GEO[f"{name}_in_faces"], offsets if offsets.size else None,
                          zb_from_file=GEO[f"{name}_in_zb"])
     g = hilbert_reorder(raw, verbose=False)[0]
-    L = build_tile_layout(g)
+    layout = build_tile_layout(g)
     order = edge_order_by_block(g.edge_cellL, 256)
     signed = remap_cell_edges(g.cell_edge_idx_signed, order).astype(np.int64)
     cell = np.repeat(np.arange(g.N), np.diff(g.cell_edge_ptr))
-    blk = cell // 256
-    local, side = L.lcsr.astype(np.int64) >> 1, L.lcsr.astype(np.int64) & 1
-    rec = L.tile_ptr[blk].astype(np.int64) + local
-    assert (local < L.tile_count[blk]).all()
-    np.testing.assert_array_equal(L.tile_edge[rec], signed >> 1)
-    np.testing.assert_array_equal(side, signed & 1)
-    np.testing.assert_array_equal(np.where(side == 1, L.tile_cr[rec], L.tile_cl[rec]), cell)
-    assert (L.tile_ptr % TILE_ALIGN == 0).all()
-    # every edge is in the tile of its left cell's block exactly once
-    owned = L.tile_edge[L.tile_edge >= 0]
-    assert np.bincount(owned, minlength=g.E).min() >= 1
-    assert L.max_tile_edges == int(L.tile_count.max())
+    for T in (layout.blocks, layout.subs):
+        tile = cell // T.tile_cells
+        local, side = T.lcsr.astype(np.int64) >> 1, T.lcsr.astype(np.int64) & 1
+        rec = T.ptr[tile].astype(np.int64) + local
+        assert (local < T.count[tile]).all()
+        np.testing.assert_array_equal(T.edge[rec], signed >> 1)
+        np.testing.assert_array_equal(side, signed & 1)
+        np.testing.assert_array_equal(np.where(side == 1, T.cr[rec], T.cl[rec]), cell)
+        assert (T.ptr % TILE_ALIGN == 0).all() and (T.lcsr_ptr % 8 == 0).all()
+        # every edge is in the tile of its left cell exactly once, and in its right cell's tile if that differs
+        assert np.bincount(T.edge[T.edge >= 0], minlength=g.E).min() >= 1
+        assert T.max_edges == int(T.count.max())
+        for t in range(T.n_tiles):
+            s0 = g.cell_edge_ptr[min(t * T.tile_cells, g.N)]
+            s1 = g.cell_edge_ptr[min((t + 1) * T.tile_cells, g.N)]
+            np.testing.assert_array_equal(T.lcsr_blk[T.lcsr_ptr[t]: T.lcsr_ptr[t] + s1 - s0], T.lcsr[s0:s1])

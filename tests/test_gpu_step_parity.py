@@ -76,15 +76,15 @@ CASES: dict[str, Callable] = {
 }
 
 
-def make_solver(grid, s: fp64_step.State, kernel: str = "staged", grid_limit: int | None = None):
+def make_solver(grid, s: fp64_step.State, kernel: str = "tiled", grid_limit: int | None = None):
     from inundation_b200.backend import SWESolverB200Resident
 
     f32 = [a.astype(np.float32) for a in (s.h, s.hu, s.hv)]
     solver = SWESolverB200Resident(grid, None, *f32, np.full(grid.N, MANNING, np.float32), dry_tol=DRY_TOL)
     solver.stage_kernel = kernel
     if grid_limit is not None:
-        # Few persistent CTAs: each loops over many blocks, so the staged kernel's
-        # prefetch of the next block overlaps the current one.
+        # Few persistent CTAs: each loops over many tiles, so the tiled kernel's
+        # prefetch of the next work item overlaps the current one.
         solver._grids = {k: min(v, grid_limit) for k, v in solver._grids.items()}
     return solver
 
@@ -112,8 +112,8 @@ def assert_same_bits(a: np.ndarray, b: np.ndarray, what: str) -> None:
     assert bad.size == 0, f"{what}: {bad.size} cells differ from the FP32 oracle (first {bad[:5].tolist()})"
 
 
-@pytest.mark.parametrize("kernel,grid_limit", [("staged", None), ("plain", None), ("staged", 5)],
-                         ids=["staged", "plain", "staged-5ctas"])
+@pytest.mark.parametrize("kernel,grid_limit", [("tiled", None), ("plain", None), ("tiled", 3), ("plain", 5)],
+                         ids=["tiled", "plain", "tiled-3ctas", "plain-5ctas"])
 @pytest.mark.parametrize("case", list(CASES))
 def test_steps_match_fp64_and_fp32_oracles(case: str, kernel: str, grid_limit, grid) -> None:
     s0 = CASES[case](grid)
