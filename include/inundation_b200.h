@@ -129,15 +129,18 @@ typedef struct {
                              1 = 256-cell blocks with plain loads */
 } swe_params_t;
 
-/* Sparse sources (device pointers): source k adds dt * rate[k] to cell
-   cells[k], times the value of hydrograph hydro[k] at its instance's clock
-   when hydro[k] != 0xFFFFFFFF. Hydrograph j is piecewise linear through the
-   knots (knot_t[i], knot_q[i]), i in [knot_ptr[j], knot_ptr[j + 1]), constant
-   outside them. */
+/* Sparse sources (device pointers), one per cell: source k adds
+   dt * rate[k] to the depth of cell cells[k] or, when hydro[k] != 0xFFFFFFFF,
+   dt * (rate[k] + hscale[k] * q), q the value of hydrograph hydro[k] at the
+   start of its instance's step (t = now_ticks / 2^20 s as a float).
+   Hydrograph j is piecewise linear through the knots (knot_t[i], knot_q[i]),
+   i in [knot_ptr[j], knot_ptr[j + 1]), and takes its end values outside them.
+   hydro == NULL: constant rates only. */
 typedef struct {
     const uint32_t *cells;
     const float *rate;
     const uint32_t *hydro;
+    const float *hscale;
     const uint32_t *knot_ptr;
     const float *knot_t;
     const float *knot_q;

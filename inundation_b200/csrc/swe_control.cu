@@ -183,9 +183,11 @@ __global__ void __launch_bounds__(kThreads) cfl_prologue_kernel(swe_mesh_t m, sw
 
 // ---------------------------------------------------------------------------
 // Sparse sources (resident.py:665-733): all increments, then the bounds.
-// A source with a hydrograph scales its rate by the hydrograph's value at the
-// start of its instance's step: t = now_ticks / 2^20 s rounded to float,
-// piecewise linear between the knots, the end values outside them.
+// A source with a hydrograph adds hscale times the hydrograph's value at the
+// start of its instance's step to its rate: t = now_ticks / 2^20 s rounded to
+// float, piecewise linear between the knots, the end values outside them.
+// (The reference's inflows are constant per phase; this is the product's own
+// interpolation, restated by the oracle.)
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float hydrograph_at(const swe_sources_t &src, uint32_t j, float t) {
     const uint32_t k0 = src.knot_ptr[j], k1 = src.knot_ptr[j + 1];
@@ -211,7 +213,8 @@ __global__ void source_apply_kernel(swe_mesh_t m, swe_state_t s, swe_sources_t s
         if (dt_bits == 0u) continue;
         const float dt = __uint_as_float(dt_bits);
         float rate = src.rate[k];
-        if (src.hydro && src.hydro[k] != 0xFFFFFFFFu) rate = rate * hydrograph_at(src, src.hydro[k], clock_seconds(s.ctrl + inst));
+        if (src.hydro && src.hydro[k] != 0xFFFFFFFFu)
+            rate = rate + src.hscale[k] * hydrograph_at(src, src.hydro[k], clock_seconds(s.ctrl + inst));
         const float inc = dt * rate;
         float h_new;
         if (comp) {
@@ -274,7 +277,8 @@ int swe_apply_sources(const swe_mesh_t *mesh, const swe_state_t *state, const sw
     if (!mesh_ok(mesh) || !state_ok(state) || !params || !sources) return SWE_ERR_ARGUMENT;
     if (sources->count == 0u) return SWE_OK;
     if (!sources->cells || !sources->rate) return SWE_ERR_ARGUMENT;
-    if (sources->hydro && (!sources->knot_ptr || !sources->knot_t || !sources->knot_q || sources->n_hydro == 0u))
+    if (sources->hydro &&
+        (!sources->hscale || !sources->knot_ptr || !sources->knot_t || !sources->knot_q || sources->n_hydro == 0u))
         return SWE_ERR_ARGUMENT;
     const uint32_t grid = min((sources->count + kThreads - 1) / kThreads, 148u * 16u);
     source_apply_kernel<<<grid, kThreads, 0, stream>>>(*mesh, *state, *sources, params->dry_tol,

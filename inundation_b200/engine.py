@@ -1,0 +1,409 @@
+"""Device state of the resident shallow-water step: one or more meshes on one B200.
+
+``ResidentEngine`` owns every device buffer (torch CUDA tensors), fills the
+C-ABI structs with their pointers and enqueues the library's kernels on its
+own stream: prologue, RETARGET, steps captured in CUDA graphs, the float64
+volume. It is the machinery under both host APIs, the reference's solver
+protocol (``backend.SWESolverB200Resident``, one mesh) and batches of
+independent meshes (``batch.BatchedSolver``). A batch is laid out by
+``layout.build_batch_layout``: every instance on whole 256-cell blocks, with
+its own clock (48-byte control block), dt words and CFL bound.
+
+There is no CPU fallback: without a CUDA device and the built library,
+construction raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+from numpy.typing import NDArray
+
+from . import native
+from .layout import TileLayout
+from .sources import NO_HYDROGRAPH, Hydrograph
+from .tuning import B200_BACKEND, CFL_DEFAULT, DRY_TOL_DEFAULT, GRAVITY_G
+
+# Host mirror of swe_ctrl_t (the reference's RESIDENT_CTRL_DTYPE, 48 bytes;
+# the reference's padding word carries the device error flag).
+RESIDENT_CTRL_DTYPE = np.dtype(
+    [
+        ("now_ticks", "<u8"),
+        ("stop_ticks", "<u8"),
+        ("steps", "<u8"),
+        ("dt_ticks", "<u4"),
+        ("dt_max_ticks", "<u4"),
+        ("dry_dt_ticks", "<u4"),
+        ("last_raw", "<f4"),
+        ("cfl_safety", "<f4"),
+        ("error", "<u4"),
+    ]
+)
+
+START, STEP, RETARGET = 0, 1, 2
+STATE_ARRAYS = ("h", "hu", "hv", "h_lo", "h1", "hu1", "hv1", "h1_lo", "clamp_mass")
+KERNELS = {"tiled": 0, "plain": 1}
+
+
+def _i32(a: NDArray) -> NDArray[np.int32]:
+    return np.ascontiguousarray(a).view(np.int32)
+
+
+class ResidentEngine:
+    """Device buffers and kernel launches of a batch of meshes (a single mesh is a batch of one)."""
+
+    default_cfl: float = CFL_DEFAULT
+    steps_per_graph: int = 200
+    active_set: bool = True
+    compensated: bool = True
+    track_clamp: bool = False
+    cfl_safety: float = 1.0
+    # Stage kernel: "tiled" (64-cell tiles from the dilation's work items, staged by bulk copies)
+    # or "plain" (256-cell blocks, direct loads).
+    stage_kernel: str = "tiled"
+
+    def _init_engine(
+        self,
+        layout: TileLayout,
+        n_mann: NDArray[np.float32],
+        *,
+        g: float = GRAVITY_G,
+        dry_tol: float = DRY_TOL_DEFAULT,
+        cfl: float | None = None,
+        device: int | str | torch.device | None = None,
+    ) -> None:
+        if not torch.cuda.is_available():
+            raise RuntimeError(f"{B200_BACKEND} needs a CUDA device; none is visible")
+        self._lib = native.load()
+        self.layout = layout
+        self.n_blocks = layout.n_blocks
+        self.n_inst = layout.n_inst
+        self._g = float(g)
+        self._dry_tol = float(dry_tol)
+        self._cfl = float(self.default_cfl if cfl is None else cfl)
+        self.device = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+        self._stream = torch.cuda.Stream(device=self.device)
+        self._upload_mesh(layout, n_mann)
+        self._alloc_state()
+        self._graphs: dict[tuple, torch.cuda.CUDAGraph] = {}
+        self._eft_checked = False
+        self._src_version = 0
+        self.clear_sources()
+
+    # -- device memory ------------------------------------------------------------------
+    def _dev(self, a: NDArray) -> torch.Tensor:
+        return torch.from_numpy(np.ascontiguousarray(a)).to(self.device)
+
+    def _upload_mesh(self, L: TileLayout, n_mann: NDArray[np.float32]) -> None:
+        B, S = L.blocks, L.subs
+        if n_mann.size != L.n_padded_cells:
+            raise ValueError(f"n_mann has {n_mann.size} values for {L.n_padded_cells} padded cells")
+        t = {"cptr": self._dev(_i32(L.cptr)), "area": self._dev(L.area),
+             "n_mann": self._dev(np.asarray(n_mann, np.float32)),
+             "ring_ptr": self._dev(_i32(L.ring_ptr)), "ring_idx": self._dev(_i32(L.ring_idx)),
+             "block_inst": self._dev(_i32(L.block_inst)), "block_cells": self._dev(_i32(L.block_cells))}
+        for prefix, T in (("tile_", B), ("sub_", S)):
+            for name in ("cl", "cr", "nx", "ny", "len", "dzl", "dzr"):
+                t[prefix + name] = self._dev(getattr(T, name))
+            t[prefix + "ptr"] = self._dev(_i32(T.ptr))
+            t[prefix + "count"] = self._dev(_i32(T.count))
+        t["lcsr"] = self._dev(B.lcsr.view(np.int16))
+        t["sub_lcsr"] = self._dev(S.lcsr_blk.view(np.int16))
+        t["sub_lcsr_ptr"] = self._dev(_i32(S.lcsr_ptr))
+        self._mesh_t = t
+        m = native.SweMesh()
+        m.n_cells = L.n_padded_cells
+        m.n_blocks = L.n_blocks
+        m.max_tile_edges = B.max_edges
+        m.n_inst = L.n_inst
+        m.max_sub_edges = S.max_edges
+        m.max_sub_slots = S.max_slots
+        for name, tensor in t.items():
+            setattr(m, name, tensor.data_ptr())
+        self._mesh = m
+        self._sms = torch.cuda.get_device_properties(self.device).multi_processor_count
+        self._per_sm: dict[int, int] = {}
+        for kernel in KERNELS.values():
+            per_sm = ctypes.c_int(0)
+            with torch.cuda.device(self.device):
+                native.check(self._lib.swe_configure(ctypes.byref(m), kernel, ctypes.byref(per_sm)), "swe_configure")
+            self._per_sm[kernel] = max(1, per_sm.value)
+        self.ctas_per_sm: int | None = None  # None: as many as fit
+        self.max_grid: int | None = None  # an upper bound on the persistent CTAs (None: none)
+
+    def grid(self, kernel: int | None = None) -> int:
+        """Persistent CTAs of a stage kernel: CTAs per SM x SMs, at most one per work unit."""
+        kernel = self._kernel if kernel is None else kernel
+        per_sm = self._per_sm[kernel] if self.ctas_per_sm is None else min(self.ctas_per_sm, self._per_sm[kernel])
+        units = 4 * self.n_blocks if kernel == 0 else self.n_blocks  # the tiled kernel works on 64-cell tiles
+        grid = min(units, per_sm * self._sms)
+        if self.max_grid is not None:
+            grid = min(grid, self.max_grid)
+        return max(1, grid)
+
+    @property
+    def _kernel(self) -> int:
+        if self.stage_kernel not in KERNELS:
+            raise ValueError(f"stage_kernel must be one of {sorted(KERNELS)}, got {self.stage_kernel!r}")
+        return KERNELS[self.stage_kernel]
+
+    def _alloc_state(self) -> None:
+        n, nb, ni, dev = self.layout.n_padded_cells, self.n_blocks, self.n_inst, self.device
+        self._t = {name: torch.zeros(n, dtype=torch.float32, device=dev) for name in STATE_ARRAYS}
+        self._blk = torch.zeros(3 * nb, dtype=torch.int32, device=dev)
+        self._active_list = torch.zeros(nb, dtype=torch.int32, device=dev)
+        self._items = torch.zeros(16 * nb, dtype=torch.int32, device=dev)  # 4 tiles x 4 words per block
+        self._sched = torch.zeros(8, dtype=torch.int64, device=dev)  # 16 uint32 words
+        dt = np.zeros(4 * ni, np.uint32)
+        dt[1::4] = np.float32(1e30).view(np.uint32)
+        self._dt_buf = self._dev(dt.view(np.int32))
+        self._ctrl_dev = torch.zeros(6 * ni, dtype=torch.int64, device=dev)
+        self._ctrl_pinned = torch.zeros(6 * ni, dtype=torch.int64).pin_memory()
+        self._ctrl = self._ctrl_pinned.numpy().view(RESIDENT_CTRL_DTYPE)
+        self._partials = torch.zeros(int(self._lib.swe_volume_partials(n)), dtype=torch.float64, device=dev)
+        self._volume = torch.zeros(1, dtype=torch.float64, device=dev)
+        s = native.SweState()
+        for name, tensor in self._t.items():
+            setattr(s, name, tensor.data_ptr())
+        s.blk = self._blk.data_ptr()
+        s.active_list = self._active_list.data_ptr()
+        s.items = self._items.data_ptr()
+        s.sched = self._sched.data_ptr()
+        s.dt_buf = self._dt_buf.data_ptr()
+        s.ctrl = self._ctrl_dev.data_ptr()
+        self._state = s
+
+    def _params(self) -> native.SweParams:
+        return native.SweParams(
+            g=self._g,
+            dry_tol=self._dry_tol,
+            cfl=self._cfl,
+            compensated=int(bool(self.compensated)),
+            track_clamp=int(bool(self.track_clamp)),
+            active_set=int(bool(self.active_set)),
+            grid=self.grid(),
+            kernel=self._kernel,
+        )
+
+    @property
+    def _cuda_stream(self) -> ctypes.c_void_p:
+        return ctypes.c_void_p(self._stream.cuda_stream)
+
+    # -- sources ----------------------------------------------------------------------
+    def clear_sources(self) -> None:
+        self._set_source_arrays(np.zeros(0, np.int64), np.zeros(0, np.float32), None, None, [])
+
+    def set_sources(
+        self,
+        rates: list[NDArray[np.float32] | None],
+        hydrographs: list[list[Hydrograph]] | None = None,
+    ) -> None:
+        """Per-instance sources: ``rates[i]`` in m^3/s per cell (the reference's
+        ``source_rate``, divided by the cell area on the way in) and inflow
+        hydrographs. One source entry per cell: a cell with both adds both.
+        """
+        L = self.layout
+        hydrographs = hydrographs or [[] for _ in range(self.n_inst)]
+        if len(rates) != self.n_inst or len(hydrographs) != self.n_inst:
+            raise ValueError(f"need sources for {self.n_inst} instances")
+        cells_all, rate_all, hidx_all, hscale_all = [], [], [], []
+        knots: list[tuple[NDArray, NDArray]] = []
+        any_hydro = False
+        for i in range(self.n_inst):
+            off, n = int(L.inst_cell_offset[i]), int(L.inst_cells[i])
+            area = L.area[off : off + n]
+            rate = np.zeros(n, np.float32)
+            if rates[i] is not None:
+                r = np.asarray(rates[i], np.float32).ravel()
+                if r.size != n:
+                    raise ValueError(f"source_rate of instance {i} has {r.size} values for {n} cells")
+                rate = r * (1.0 / area).astype(np.float32)
+            hidx = np.full(n, NO_HYDROGRAPH, np.uint32)
+            hscale = np.zeros(n, np.float32)
+            for hg in hydrographs[i]:
+                hg.validate(n)
+                cells = np.asarray(hg.cells, np.int64).ravel()
+                if (hidx[cells] != NO_HYDROGRAPH).any():
+                    raise ValueError("two hydrographs share a cell")
+                hidx[cells] = len(knots)
+                hscale[cells] = hg.shares() * (1.0 / area[cells]).astype(np.float32)
+                knots.append((np.asarray(hg.knot_t, np.float32).ravel(), np.asarray(hg.knot_q, np.float32).ravel()))
+                any_hydro = True
+            live = np.flatnonzero((rate != 0) | (hidx != NO_HYDROGRAPH))
+            cells_all.append(live + off)
+            rate_all.append(rate[live])
+            hidx_all.append(hidx[live])
+            hscale_all.append(hscale[live])
+        self._set_source_arrays(
+            np.concatenate(cells_all),
+            np.concatenate(rate_all),
+            np.concatenate(hidx_all) if any_hydro else None,
+            np.concatenate(hscale_all) if any_hydro else None,
+            knots,
+        )
+
+    def _set_source_arrays(self, cells, rate, hidx, hscale, knots) -> None:
+        dev = self._dev
+        self._src_count = int(cells.size)
+        self._src_cells = dev(cells.astype(np.int32) if cells.size else np.zeros(1, np.int32))
+        self._src_rate = dev(rate.astype(np.float32) if cells.size else np.zeros(1, np.float32))
+        self._src_hydro = None
+        if hidx is not None and knots:
+            ptr = np.zeros(len(knots) + 1, np.int64)
+            np.cumsum([t.size for t, _ in knots], out=ptr[1:])
+            self._src_hydro = {
+                "hydro": dev(hidx.view(np.int32)),
+                "hscale": dev(hscale.astype(np.float32)),
+                "knot_ptr": dev(ptr.astype(np.int32)),
+                "knot_t": dev(np.concatenate([t for t, _ in knots])),
+                "knot_q": dev(np.concatenate([q for _, q in knots])),
+                "n": len(knots),
+            }
+        self._src_version += 1
+
+    def _sources(self) -> native.SweSources:
+        s = native.SweSources(cells=self._src_cells.data_ptr(), rate=self._src_rate.data_ptr(), count=self._src_count)
+        if self._src_hydro is not None:
+            h = self._src_hydro
+            for name in ("hydro", "hscale", "knot_ptr", "knot_t", "knot_q"):
+                setattr(s, name, h[name].data_ptr())
+            s.n_hydro = h["n"]
+        return s
+
+    # -- state access ---------------------------------------------------------------------
+    def _inst_range(self, inst: int) -> slice:
+        off = int(self.layout.inst_cell_offset[inst])
+        return slice(off, off + int(self.layout.inst_cells[inst]))
+
+    def download_state(self, name: str, inst: int = 0) -> NDArray[np.float32]:
+        with torch.cuda.stream(self._stream):
+            out = self._t[name][self._inst_range(inst)].cpu().numpy()
+        return out.copy()
+
+    def upload_state(self, name: str, values: NDArray[np.float32], inst: int = 0) -> None:
+        src = torch.from_numpy(np.ascontiguousarray(values, np.float32).ravel())
+        with torch.cuda.stream(self._stream):
+            self._t[name][self._inst_range(inst)].copy_(src)
+        self._stream.synchronize()
+
+    def download_block_flags(self) -> NDArray[np.uint32]:
+        """``(n_blocks, 3)`` flags: wet, active, forced."""
+        with torch.cuda.stream(self._stream):
+            words = self._blk.cpu().numpy()
+        return words.view(np.uint32).reshape(self.n_blocks, 3).copy()
+
+    def volume_fp64(self, inst: int = 0) -> float:
+        """Sum of (h + h_lo) * area of one instance in float64 on the device, in a fixed order."""
+        r = self._inst_range(inst)
+        off, n = r.start, r.stop - r.start
+        with torch.cuda.stream(self._stream):
+            native.check(
+                self._lib.swe_volume_fp64(
+                    self._t["h"][off:].data_ptr(), self._t["h_lo"][off:].data_ptr(),
+                    self._mesh_t["area"][off:].data_ptr(), n, self._partials.data_ptr(), self._volume.data_ptr(),
+                    self._cuda_stream,
+                ),
+                "swe_volume_fp64",
+            )
+            out = float(self._volume.cpu().item())
+        return out
+
+    @property
+    def computed_cells(self) -> int:
+        """Cells in computed tiles summed over all real steps (the roofline's cell-step count)."""
+        self._stream.synchronize()
+        return int(self._sched.cpu().numpy().view(np.uint64)[3])
+
+    # -- kernels ----------------------------------------------------------------------------------
+    def _check_error_free_arithmetic(self) -> None:
+        if self._eft_checked:
+            return
+        v = torch.tensor([1.0, 1e-9, 0.0], dtype=torch.float32, device=self.device)
+        with torch.cuda.stream(self._stream):
+            native.check(self._lib.swe_eft_probe(v.data_ptr(), self._cuda_stream), "swe_eft_probe")
+            got = v.cpu().numpy()
+        if float(got[2]) != float(np.float32(1e-9)):
+            raise RuntimeError("error-free arithmetic is broken on this device, so compensated depth would leak mass")
+        self._eft_checked = True
+
+    def _sync_ctrl_to_device(self) -> None:
+        with torch.cuda.stream(self._stream):
+            self._ctrl_dev.copy_(self._ctrl_pinned, non_blocking=True)
+
+    def _read_ctrl(self) -> None:
+        with torch.cuda.stream(self._stream):
+            self._ctrl_pinned.copy_(self._ctrl_dev, non_blocking=True)
+        self._stream.synchronize()
+        err = int(self._ctrl["error"].max())
+        if err:
+            raise RuntimeError(f"{B200_BACKEND}: a bounded device wait for staged data timed out (error {err})")
+
+    def _enqueue_prologue(self) -> None:
+        p = self._params()
+        with torch.cuda.stream(self._stream):
+            self._sched[:3].zero_()  # list counters; words 6-7 keep the computed-cells total
+            self._sched[4:].zero_()
+            native.check(
+                self._lib.swe_prologue(
+                    ctypes.byref(self._mesh), ctypes.byref(self._state), ctypes.byref(p), self._cuda_stream
+                ),
+                "swe_prologue",
+            )
+
+    def _enqueue_retarget(self) -> None:
+        """RETARGET every clock to its new stop, rebuilding the active lists first.
+
+        A no-op step leaves its instance out of the lists, so the lists are
+        rebuilt by a forced dilation (the flags come out the same: they were
+        dilated from the same wet marks after the last real step).
+        """
+        p = self._params()
+        with torch.cuda.stream(self._stream):
+            native.check(
+                self._lib.swe_block_dilate_compact(
+                    ctypes.byref(self._mesh), ctypes.byref(self._state), ctypes.byref(p), 1, RETARGET,
+                    self._cuda_stream,
+                ),
+                "swe_block_dilate_compact",
+            )
+
+    def _enqueue_steps(self, n_steps: int, params: native.SweParams, sources: native.SweSources) -> None:
+        mesh, state = ctypes.byref(self._mesh), ctypes.byref(self._state)
+        pp, sp = ctypes.byref(params), ctypes.byref(sources)
+        stream = ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+        for _ in range(n_steps):
+            native.check(self._lib.swe_step(mesh, state, pp, sp, stream), "swe_step")
+
+    def _graph(self, steps: int | None = None) -> torch.cuda.CUDAGraph:
+        steps = self.steps_per_graph if steps is None else steps
+        key = (
+            steps,
+            bool(self.compensated),
+            bool(self.track_clamp),
+            bool(self.active_set),
+            self._kernel,
+            self.grid(),
+            self._src_version,
+        )
+        graph = self._graphs.get(key)
+        if graph is None:
+            params, sources = self._params(), self._sources()
+            graph = torch.cuda.CUDAGraph()
+            self._stream.synchronize()
+            with torch.cuda.graph(graph, stream=self._stream):
+                self._enqueue_steps(steps, params, sources)
+            while len(self._graphs) >= 4:  # keep the few most recent graphs alive
+                self._graphs.pop(next(iter(self._graphs)))
+            self._graphs[key] = graph
+        return graph
+
+    def step_graph(self) -> None:
+        """Replay one submit of ``steps_per_graph`` steps (no host sync)."""
+        graph = self._graph()
+        with torch.cuda.stream(self._stream):
+            graph.replay()
+
+
+__all__ = ["KERNELS", "NO_HYDROGRAPH", "RESIDENT_CTRL_DTYPE", "Hydrograph", "ResidentEngine", "START", "STEP", "RETARGET"]

@@ -73,6 +73,14 @@ class TileLayout:
     ring_ptr: NDArray[np.uint32]
     ring_idx: NDArray[np.uint32]
     area: NDArray[np.float32]  # padded to n_blocks * 256 with 1.0
+    block_inst: NDArray[np.uint32]  # instance of every block (all 0 for one mesh)
+    block_cells: NDArray[np.uint32]  # real cells of every block
+    inst_cell_offset: NDArray[np.int64]  # first cell of every instance (a multiple of 256)
+    inst_cells: NDArray[np.int64]  # real cells of every instance
+
+    @property
+    def n_inst(self) -> int:
+        return int(self.inst_cells.size)
 
     @property
     def n_padded_cells(self) -> int:
@@ -81,12 +89,6 @@ class TileLayout:
     @property
     def max_tile_edges(self) -> int:
         return self.blocks.max_edges
-
-    @property
-    def block_cells(self) -> NDArray[np.uint32]:
-        """Real cells of every 256-cell block (the last one may be partial)."""
-        first = np.arange(self.n_blocks, dtype=np.int64) * ACTIVE_BLOCK_CELLS
-        return np.minimum(ACTIVE_BLOCK_CELLS, self.n_cells - first).astype(np.uint32)
 
     @property
     def foreign_edges(self) -> int:
@@ -175,6 +177,15 @@ def _tile_set(geom: MeshGeometry, order: NDArray[np.int64], signed: NDArray[np.i
 
 def build_tile_layout(geom: MeshGeometry) -> TileLayout:
     """Both tile sets, the padded CSR pointers and the block two-ring of a Hilbert-ordered geometry."""
+    n = int(geom.N)
+    layout = _build(geom)
+    first = np.arange(layout.n_blocks, dtype=np.int64) * ACTIVE_BLOCK_CELLS
+    layout.block_cells = np.minimum(ACTIVE_BLOCK_CELLS, n - first).astype(np.uint32)
+    layout.inst_cells = np.array([n], dtype=np.int64)
+    return layout
+
+
+def _build(geom) -> TileLayout:
     n, n_e = int(geom.N), int(geom.E)
     if n == 0 or n_e == 0:
         raise ValueError("mesh has no cells or no edges")
@@ -201,10 +212,90 @@ def build_tile_layout(geom: MeshGeometry) -> TileLayout:
         ring_ptr=rptr.astype(np.uint32),
         ring_idx=ridx.astype(np.uint32) if ridx.size else np.zeros(1, np.uint32),
         area=np.concatenate([geom.area.astype(np.float32), np.ones(n_blk * bc - n, np.float32)]),
+        block_inst=np.zeros(n_blk, np.uint32),
+        block_cells=np.full(n_blk, bc, np.uint32),
+        inst_cell_offset=np.zeros(1, np.int64),
+        inst_cells=np.array([n], np.int64),
     )
 
 
-def algorithmic_bytes_per_cell_step(geom: MeshGeometry) -> float:
+@dataclass
+class _Concatenated:
+    """The fields of ``MeshGeometry`` the layout reads, for a batch of meshes."""
+
+    N: int
+    E: int
+    edge_cellL: NDArray[np.int32]
+    edge_cellR: NDArray[np.int32]
+    edge_nx: NDArray[np.float32]
+    edge_ny: NDArray[np.float32]
+    edge_len: NDArray[np.float32]
+    edge_dzL: NDArray[np.float32]
+    edge_dzR: NDArray[np.float32]
+    cell_edge_ptr: NDArray[np.int64]
+    cell_edge_idx_signed: NDArray[np.int64]
+    area: NDArray[np.float32]
+
+
+def build_batch_layout(geoms: list[MeshGeometry]) -> TileLayout:
+    """One layout for a batch of independent Hilbert-ordered meshes.
+
+    Instance ``i`` takes whole blocks from cell ``inst_cell_offset[i]``; the
+    cells that pad its last block have no edges and are never updated. Every
+    instance keeps the tiles, edge segments and per-cell CSR order it has on
+    its own, so its results are bit-identical to a run of that mesh alone.
+    """
+    if not geoms:
+        raise ValueError("a batch needs at least one mesh")
+    bc = ACTIVE_BLOCK_CELLS
+    sizes = np.array([int(g.N) for g in geoms], dtype=np.int64)
+    padded = (sizes + bc - 1) // bc * bc
+    offs = np.zeros(len(geoms) + 1, dtype=np.int64)
+    np.cumsum(padded, out=offs[1:])
+    e_offs = np.zeros(len(geoms) + 1, dtype=np.int64)
+    np.cumsum([int(g.E) for g in geoms], out=e_offs[1:])
+    total = int(offs[-1])
+    ptr = np.zeros(total + 1, dtype=np.int64)
+    area = np.ones(total, dtype=np.float32)
+    signed, cl, cr = [], [], []
+    for i, g in enumerate(geoms):
+        o, n = int(offs[i]), int(g.N)
+        gptr = g.cell_edge_ptr.astype(np.int64)
+        ptr[o + 1 : o + n + 1] = ptr[o] + gptr[1:]
+        ptr[o + n + 1 : int(offs[i + 1]) + 1] = ptr[o] + gptr[-1]
+        area[o : o + n] = g.area
+        signed.append(g.cell_edge_idx_signed.astype(np.int64) + 2 * int(e_offs[i]))
+        cl.append(g.edge_cellL.astype(np.int64) + o)
+        r = g.edge_cellR.astype(np.int64)
+        cr.append(np.where(r >= 0, r + o, r))
+    cat = lambda name: np.concatenate([getattr(g, name) for g in geoms]).astype(np.float32)  # noqa: E731
+    geom = _Concatenated(
+        N=total,
+        E=int(e_offs[-1]),
+        edge_cellL=np.concatenate(cl).astype(np.int32),
+        edge_cellR=np.concatenate(cr).astype(np.int32),
+        edge_nx=cat("edge_nx"),
+        edge_ny=cat("edge_ny"),
+        edge_len=cat("edge_len"),
+        edge_dzL=cat("edge_dzL"),
+        edge_dzR=cat("edge_dzR"),
+        cell_edge_ptr=ptr,
+        cell_edge_idx_signed=np.concatenate(signed),
+        area=area,
+    )
+    layout = _build(geom)
+    blocks = padded // bc
+    layout.block_inst = np.repeat(np.arange(len(geoms), dtype=np.uint32), blocks)
+    cells = np.full(layout.n_blocks, bc, dtype=np.int64)
+    last = np.cumsum(blocks) - 1
+    cells[last] = sizes - (blocks - 1) * bc
+    layout.block_cells = cells.astype(np.uint32)
+    layout.inst_cell_offset = offs[:-1].copy()
+    layout.inst_cells = sizes
+    return layout
+
+
+def algorithmic_bytes_per_cell_step(geom: MeshGeometry | list[MeshGeometry]) -> float:
     """Compulsory HBM bytes of one Heun step per cell.
 
     Per stage: edge geometry 28 B per edge (cL, cR, nx, ny, len, dzL, dzR),
@@ -212,6 +303,8 @@ def algorithmic_bytes_per_cell_step(geom: MeshGeometry) -> float:
     the predictor reads U^n and writes U* (32 B), the corrector reads U* and
     U^n and writes U^{n+1} (48 B). B = 2 (28 E/N + 12 + 4 S/N) + 80.
     """
-    e_per_n = geom.E / geom.N
-    s_per_n = float(geom.cell_edge_ptr[-1]) / geom.N
+    geoms = geom if isinstance(geom, list) else [geom]
+    n = sum(int(g.N) for g in geoms)
+    e_per_n = sum(int(g.E) for g in geoms) / n
+    s_per_n = sum(float(g.cell_edge_ptr[-1]) for g in geoms) / n
     return 2.0 * (28.0 * e_per_n + 12.0 + 4.0 * s_per_n) + 80.0

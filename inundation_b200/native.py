@@ -87,7 +87,7 @@ class SweParams(ctypes.Structure):
 
 class SweSources(ctypes.Structure):
     _fields_ = [
-        *[(name, _P) for name in ("cells", "rate", "hydro", "knot_ptr", "knot_t", "knot_q")],
+        *[(name, _P) for name in ("cells", "rate", "hydro", "hscale", "knot_ptr", "knot_t", "knot_q")],
         ("count", _U32),
         ("n_hydro", _U32),
     ]

@@ -13,7 +13,7 @@ name.
 * ``rain_inflow``   -- 4M cells, 40 m relief, n log-uniform in [0.02, 0.08], 50 mm/h rain
   for 30 min and a triangular 200 m^3/s inflow peaking at 20 min, initially dry.
 * ``batch_member``  -- one of the batched scenarios: N cells, own DEM, n in
-  [0.02, 0.06], triangular inflow of 10-300 m^3/s.
+  [0.02, 0.06], triangular inflow of 10-300 m^3/s peaking at 20 min, initially dry.
 """
 
 from __future__ import annotations
@@ -25,6 +25,7 @@ from numpy.typing import NDArray
 
 from .mesh.geometry import MeshGeometry, build_geometry, hilbert_reorder, with_bed
 from .mesh.synthetic import carve_channel, fractal_dem, gaussian_bumps, voronoi_mesh
+from .sources import Hydrograph, triangular_knots
 from .tuning import DRY_TOL_DEFAULT
 
 
@@ -40,8 +41,12 @@ class Scenario:
     dt_max: float = 1.0
     dt_init: float = 0.01
     dry_tol: float = DRY_TOL_DEFAULT
-    # Piecewise-constant per-cell source rates [m^3/s]: (start time, rate array).
+    # Piecewise-constant per-cell source rates [m^3/s]: (start time, rate array), the
+    # reference's phase form of the sources.
     source_phases: list[tuple[float, NDArray[np.float32]]] = field(default_factory=list)
+    # The same sources in the device form: constant per-cell rates [m^3/s] plus hydrographs.
+    source_rate: NDArray[np.float32] | None = None
+    hydrographs: list[Hydrograph] = field(default_factory=list)
     meta: dict = field(default_factory=dict)
 
     @property
@@ -109,7 +114,10 @@ def rain_inflow(n_cells: int = 4_000_000, seed: int = 3, side: float = 20_000.0,
         rate = (rain * area).astype(np.float32)
         rate[inflow_cell] += np.float32(triangular_hydrograph(t_mid, 200.0, 1200.0, 1800.0))
         phases.append((k * phase_s, rate))
+    kt, kq = triangular_knots(200.0, 1200.0, 1800.0)
+    inflow = Hydrograph(cells=np.array([inflow_cell]), knot_t=kt, knot_q=kq)
     return Scenario("rain_inflow", geom, z.copy(), z.copy(), z.copy(), manning, t_end=1800.0, source_phases=phases,
+                    source_rate=(rain * area).astype(np.float32), hydrographs=[inflow],
                     meta={"rain_m_per_s": rain, "inflow_cell": inflow_cell, "peak_m3s": 200.0})
 
 
@@ -122,7 +130,9 @@ def batch_member(n_cells: int, seed: int, spacing: float = 10.0) -> Scenario:
     peak = float(rng.uniform(10.0, 300.0))
     z = np.zeros(geom.N, np.float32)
     cell = int(np.argmax(geom.zb))
-    return Scenario("batch_member", geom, z.copy(), z.copy(), z.copy(), manning, t_end=3600.0,
+    kt, kq = triangular_knots(peak, 1200.0, 1800.0)
+    inflow = Hydrograph(cells=np.array([cell]), knot_t=kt, knot_q=kq)
+    return Scenario("batch_member", geom, z.copy(), z.copy(), z.copy(), manning, t_end=1800.0, hydrographs=[inflow],
                     meta={"inflow_cell": cell, "peak_m3s": peak})
 
 

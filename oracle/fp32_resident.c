@@ -75,6 +75,12 @@ typedef struct {
     uint32_t *dt_buf; /* [0] this step's dt bits, [1] next step's CFL bound bits */
     float *clamp_mass;
     ctrl_t *ctrl;
+    /* Inflow hydrographs of the sources (src_hydro NULL: constant rates). */
+    const uint32_t *src_hydro;
+    const float *src_hscale;
+    const uint32_t *knot_ptr;
+    const float *knot_t;
+    const float *knot_q;
 } oracle_t;
 
 static inline uint32_t fbits(float f) { uint32_t u; memcpy(&u, &f, 4); return u; }
@@ -341,12 +347,31 @@ void oracle_update_stage(oracle_t *o, int stage, int compensated, int track_clam
 }
 
 /* Sources as (cell, dh/dt) pairs: all increments first, then the bounds. */
+/* A source's hydrograph value at clock t (seconds): piecewise linear between
+   the knots, the end values outside them. Not in the reference, whose inflows
+   are constant per phase; the product evaluates the same expression at the
+   start of every step, t = now_ticks / 2^20 rounded to float. */
+static float hydrograph_at(const oracle_t *o, uint32_t j, float t) {
+    uint32_t k0 = o->knot_ptr[j], k1 = o->knot_ptr[j + 1u];
+    if (k1 <= k0) return 0.0f;
+    if (!(t > o->knot_t[k0])) return o->knot_q[k0];
+    if (!(t < o->knot_t[k1 - 1u])) return o->knot_q[k1 - 1u];
+    uint32_t k = k0;
+    while (k + 2u < k1 && !(t < o->knot_t[k + 1u])) ++k;
+    float t0 = o->knot_t[k], t1 = o->knot_t[k + 1u];
+    float q0 = o->knot_q[k], q1 = o->knot_q[k + 1u];
+    return q0 + (q1 - q0) * ((t - t0) / (t1 - t0));
+}
+
 void oracle_sources(oracle_t *o, const uint32_t *cells, const float *rate, uint32_t count, int compensated) {
     if (o->dt_buf[0] == 0u) return;
     float dt = bitsf(o->dt_buf[0]);
+    float t = (float)o->ctrl->now_ticks * (1.0f / 1048576.0f);
     for (uint32_t k = 0; k < count; ++k) {
         uint32_t i = cells[k];
-        float inc = dt * rate[k];
+        float r = rate[k];
+        if (o->src_hydro && o->src_hydro[k] != 0xFFFFFFFFu) r = r + o->src_hscale[k] * hydrograph_at(o, o->src_hydro[k], t);
+        float inc = dt * r;
         float h_new;
         if (compensated) {
             float lo_new;

@@ -101,6 +101,7 @@ class _Oracle(ctypes.Structure):
         *[(name, ctypes.c_void_p) for name in (
             "ecL", "ecR", "enx", "eny", "elen", "edz", "area", "n_mann", "cptr", "cidx", "erange", "bptr", "bidx",
             "h", "hu", "hv", "h1", "hu1", "hv1", "h_lo", "h1_lo", "ef", "touched", "blk", "dt_buf", "clamp_mass", "ctrl",
+            "src_hydro", "src_hscale", "knot_ptr", "knot_t", "knot_q",
         )],
     ]
 
@@ -203,15 +204,43 @@ class ResidentOracle:
         a["h1_lo"][:] = 0.0
 
     # -- kernels --------------------------------------------------------------------
-    def set_sources(self, source_rate: np.ndarray | None) -> None:
-        if source_rate is None:
-            self._n_src = 0
-            return
-        per_sec = np.asarray(source_rate, np.float32) * (1.0 / self.arrays["area"]).astype(np.float32)
-        cells = np.flatnonzero(per_sec).astype(np.uint32)
+    def set_sources(self, source_rate: np.ndarray | None, hydrographs: list | None = None) -> None:
+        """Constant rates (m^3/s per cell) and inflow hydrographs, one entry per cell.
+
+        A hydrograph has ``cells``, ``knot_t``, ``knot_q`` and optional ``share``
+        (equal parts by default): cell k gains ``share[k] * q(t) / area`` m/s.
+        """
+        area = self.arrays["area"]
+        rate = np.zeros(self.N, np.float32)
+        if source_rate is not None:
+            rate = np.asarray(source_rate, np.float32) * (1.0 / area).astype(np.float32)
+        hidx = np.full(self.N, 0xFFFFFFFF, np.uint32)
+        hscale = np.zeros(self.N, np.float32)
+        knots_t, knots_q, ptr = [], [], [0]
+        for j, hg in enumerate(hydrographs or []):
+            cells = np.asarray(hg.cells, np.int64).ravel()
+            share = (np.full(cells.size, 1.0 / cells.size, np.float32) if getattr(hg, "share", None) is None
+                     else np.asarray(hg.share, np.float32).ravel())
+            hidx[cells] = j
+            hscale[cells] = share * (1.0 / area[cells]).astype(np.float32)
+            knots_t.append(np.asarray(hg.knot_t, np.float32).ravel())
+            knots_q.append(np.asarray(hg.knot_q, np.float32).ravel())
+            ptr.append(ptr[-1] + knots_t[-1].size)
+        cells = np.flatnonzero((rate != 0) | (hidx != 0xFFFFFFFF)).astype(np.uint32)
         self._src_cells = cells if cells.size else np.zeros(1, np.uint32)
-        self._src_rate = per_sec[cells].astype(np.float32) if cells.size else np.zeros(1, np.float32)
+        self._src_rate = rate[cells].astype(np.float32) if cells.size else np.zeros(1, np.float32)
         self._n_src = int(cells.size)
+        self._hydro = None
+        if knots_t and cells.size:
+            self._hydro = {
+                "src_hydro": np.ascontiguousarray(hidx[cells]),
+                "src_hscale": np.ascontiguousarray(hscale[cells]),
+                "knot_ptr": np.asarray(ptr, np.uint32),
+                "knot_t": np.concatenate(knots_t),
+                "knot_q": np.concatenate(knots_q),
+            }
+        for name in ("src_hydro", "src_hscale", "knot_ptr", "knot_t", "knot_q"):
+            setattr(self._struct, name, _ptr(self._hydro[name]) if self._hydro else None)
 
     def prologue(self) -> None:
         L = lib()
@@ -248,6 +277,7 @@ class ResidentOracle:
         source_rate: np.ndarray | None = None,
         resume: bool = False,
         t_start: float = 0.0,
+        hydrographs: list | None = None,
     ) -> tuple[list[np.ndarray], list[float]]:
         """The reference's window loop (gpu_resident_batch.py:648-762), on the C kernels.
 
@@ -261,7 +291,7 @@ class ResidentOracle:
         interval = seconds_to_ticks(output_interval_s)
         if not resume:
             self.reset()
-        self.set_sources(source_rate)
+        self.set_sources(source_rate, hydrographs)
         snaps = [self.download_h()]
         times = [ticks_to_seconds(start)]
         c = self.ctrl

@@ -85,7 +85,7 @@ def make_solver(grid, s: fp64_step.State, kernel: str = "tiled", grid_limit: int
     if grid_limit is not None:
         # Few persistent CTAs: each loops over many tiles, so the tiled kernel's
         # prefetch of the next work item overlaps the current one.
-        solver._grids = {k: min(v, grid_limit) for k, v in solver._grids.items()}
+        solver.max_grid = grid_limit
     return solver
 
 
