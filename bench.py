@@ -61,6 +61,9 @@ def parse_args() -> argparse.Namespace:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--chunk", type=int, default=500, help="steps per captured graph in the timed region")
     ap.add_argument("--kernel", choices=["tiled", "plain"], default="tiled", help="stage kernel variant")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-scenarios measurement")
+    ap.add_argument("--batch-count", type=int, default=64, help="scenarios in the batched measurement")
+    ap.add_argument("--batch-steps", type=int, default=2000, help="steps of every scenario in the batched measurement")
     return ap.parse_args()
 
 
@@ -400,6 +403,10 @@ def run_b200(args, world: int, rank: int, local: int) -> None:
         cpu, err = cpu_baseline_and_error(sc, SWESolverB200Resident, device)
         line["cpu_baseline"] = cpu
         line["fp64_oracle_error"] = err
+    del solver
+    torch.cuda.empty_cache()
+    if not args.no_batch:
+        line["batched"] = run_batch(args, world, local)
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -431,6 +438,156 @@ def e2e_run(solver, sc, t_sim: float, args) -> dict:
         "h2d_bytes_per_step": (12 * n + 48) / steps,
         "d2h_bytes_per_step": (24 * n + 48 * (submits + 1)) / steps,
         "path": "SWESolverB200Resident.reset(host h, hu, hv) + run(t_end) + download_h/hu/hv",
+    }
+
+
+# -- batched scenarios -------------------------------------------------------------------------------
+def _batch_scenario(n_seed: tuple[int, int]):
+    os.environ["OMP_NUM_THREADS"] = "1"
+    sys.path.insert(0, str(ROOT))
+    from inundation_b200 import scenarios
+
+    return scenarios.batch_member(*n_seed)
+
+
+def build_batch(count: int) -> list:
+    """The batched workload: ``count`` seeded scenarios, N log-uniform in [20k, 500k], built in parallel."""
+    import multiprocessing as mp
+
+    from inundation_b200 import scenarios
+
+    sizes = scenarios.batch_sizes(count)
+    jobs = [(n, 1000 + i) for i, n in enumerate(sizes)]
+    procs = max(1, min(os.cpu_count() or 1, 16, count))
+    with mp.get_context("spawn").Pool(procs) as pool:
+        return pool.map(_batch_scenario, jobs, chunksize=1)
+
+
+def _timed_steps(solver, steps: int, graph_steps: int) -> float:
+    """Device milliseconds of ``steps`` steps replayed as graphs of ``graph_steps`` (captured beforehand)."""
+    import torch
+
+    solver.steps_per_graph = graph_steps
+    full, rest = divmod(steps, graph_steps)
+    graphs = ([solver._graph()] * full) + ([solver._graph(rest)] if rest else [])
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(solver._stream):
+        ev0.record(solver._stream)
+        for g in graphs:
+            g.replay()
+        ev1.record(solver._stream)
+    ev1.synchronize()
+    return ev0.elapsed_time(ev1)
+
+
+def run_batch(args, world: int, local: int) -> dict:
+    """Batched forward against the same scenarios run one at a time (both on this GPU).
+
+    Every scenario: a seeded Voronoi mesh of N cells (log-uniform in
+    [20k, 500k]) at 10 m spacing on its own fractal DEM, n uniform in
+    [0.02, 0.06], initially dry, fed by a triangular inflow hydrograph
+    (peak 10-300 m^3/s at 20 min) at its highest cell; ``--batch-steps``
+    steps each, every scenario with its own CFL dt.
+    """
+    import torch
+
+    from inundation_b200.batch import BatchedSolver, BatchMember, autotune
+    from inundation_b200.layout import algorithmic_bytes_per_cell_step
+
+    t_build = time.perf_counter()
+    scs = build_batch(args.batch_count)
+    t_build = time.perf_counter() - t_build
+    members = [BatchMember(s.geom, s.h0, s.hu0, s.hv0, s.manning, hydrographs=s.hydrographs) for s in scs]
+    cells = int(sum(s.geom.N for s in scs))
+    steps = args.batch_steps
+    dt_max, dt_init = scs[0].dt_max, scs[0].dt_init
+    device = f"cuda:{local}"
+
+    solver = BatchedSolver(members, device=device)
+    tune = autotune(solver, dt_max=dt_max, dt_init=dt_init, steps=40)
+    solver.reset()
+    solver.start(dt_max, dt_init)
+    _timed_steps(solver, args.warmup, max(1, args.warmup))  # warm-up steps, not timed
+    computed0 = solver.computed_cells
+    steps0 = solver.steps.copy()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms = _timed_steps(solver, steps, 200)
+    clock = clocks.stop()
+    done = solver.steps - steps0
+    if not (done == steps).all():
+        raise RuntimeError(f"batched run: scenarios ran {sorted(set(done.tolist()))} steps, expected {steps}")
+    computed = solver.computed_cells - computed0
+    ms_max = reduce_max(ms, world)
+    bpc = algorithmic_bytes_per_cell_step([s.geom for s in scs])
+    peak, peak_kind = peaks()
+
+    # End to end through the public calls: host initial states in, final depths out.
+    t0 = time.perf_counter()
+    solver.reset()
+    solver.start(dt_max, dt_init)
+    solver.run_steps(steps)
+    finals = [solver.download_h(i) for i in range(solver.n_inst)]
+    n_done = solver.steps
+    e2e_wall = time.perf_counter() - t0
+    if not (n_done == steps).all():
+        raise RuntimeError("batched end-to-end run stalled")
+    del finals
+    kernel = solver.stage_kernel
+    launches_per_step = 3 + (2 if solver._src_count else 0)  # stages, dilation (+ source increments and bounds)
+    del solver
+    torch.cuda.empty_cache()
+
+    # The same scenarios one at a time, each with its own solver and graphs.
+    plain_ms = 0.0
+    plain_computed = 0
+    for m in members:
+        one = BatchedSolver([m], device=device)
+        one.stage_kernel = kernel
+        one.start(dt_max, dt_init)
+        _timed_steps(one, args.warmup, max(1, args.warmup))
+        c0 = one.computed_cells
+        plain_ms += _timed_steps(one, steps, 200)
+        plain_computed += one.computed_cells - c0
+        del one
+    torch.cuda.empty_cache()
+    value = world * cells * steps / (ms_max * 1e-3)
+    achieved = computed * bpc / (ms * 1e-3) / 1e9
+    return {
+        "workload": f"batch{args.batch_count}_voronoi_inflow",
+        "scenarios": args.batch_count,
+        "cells": cells,
+        "steps_per_scenario": steps,
+        "value": value,
+        "unit": UNIT,
+        "ms_per_step": ms_max / steps,
+        "computed_cell_steps_per_s": world * computed / (ms_max * 1e-3),
+        "active_fraction": computed / (cells * steps),
+        "achieved_gbs_over_step": achieved,
+        "hbm_frac_of_step": achieved / peak,
+        "peak_kind": f"{peak_kind} HBM copy bandwidth",
+        "plain": {
+            "value": cells * steps / (plain_ms * 1e-3),
+            "ms_total": plain_ms,
+            "computed_cell_steps_per_s": plain_computed / (plain_ms * 1e-3),
+            "note": "each scenario alone through the same kernels, one after another",
+        },
+        "speedup_vs_plain": plain_ms / ms,
+        "autotune": {"stage_kernel": tune["stage_kernel"], "ctas_per_sm": tune["ctas_per_sm"],
+                     "candidates": [(r["stage_kernel"], r["ctas_per_sm"], round(r["ms_per_step"], 5))
+                                    for r in tune["results"]]},
+        "e2e": {
+            "value": cells * steps / e2e_wall,
+            "unit": UNIT,
+            "wall_s": e2e_wall,
+            "h2d_bytes_per_step": (12 * cells + 48 * args.batch_count) / steps,
+            "d2h_bytes_per_step": (4 * cells + 2 * 48 * args.batch_count) / steps,
+            "path": "BatchedSolver.reset(host states) + start + run_steps + download_h per scenario",
+        },
+        "build_s": t_build,
+        "gpu_launches": launches_per_step * steps,
+        "clocks": clock,
     }
 
 
