@@ -205,6 +205,76 @@ int swe_prologue(const swe_mesh_t *mesh, const swe_state_t *state, const swe_par
 int swe_step(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params_t *params,
              const swe_sources_t *sources, swe_stream_t stream);
 
+/* ---- Adjoint: gradients of a gauge misfit, dt frozen ------------------------------------------
+   No counterpart in the reference. The loss is sum over steps n = 1..N and
+   gauges g of ((h + h_lo)(g, after step n) - obs[n - 1][g])^2; its gradient
+   is taken with respect to Manning's n and the bed of every cell and to the
+   discharge knots of the inflow hydrographs, with every step's dt held at
+   its forward value. A run keeps checkpoints; each segment of steps is run
+   again with swe_tape_record + swe_stage_taped to fill the tape, then
+   reversed one step at a time by swe_adjoint_step (single-instance meshes). */
+
+/* The record of a segment of steps (device pointers; slot k = k-th step of
+   the segment, n = n_blocks * 256 padded cells). */
+typedef struct {
+    float *h, *hu, *hv, *h_lo; /* (capacity + 1) x n: the state at the start of every step, then at the end */
+    float *s0, *s1;            /* capacity x 3 x n: each stage's gathered sums (sdh, sdhu, sdhv) */
+    uint32_t *dt;              /* capacity: dt bits of every step (0 = a no-op step) */
+    float *t;                  /* capacity: the hydrograph clock of every step, seconds */
+    uint32_t *list;            /* capacity x n_blocks: the active blocks of every step */
+    uint32_t *count;           /* capacity */
+    uint32_t capacity;
+} swe_tape_t;
+
+/* Adjoint state and gradients (device pointers, n padded cells). */
+typedef struct {
+    float *lh, *lhu, *lhv;      /* adjoint of the state, carried from step to step */
+    float *ls;                  /* 3 x n: adjoint of a stage's sums (scratch) */
+    float *lsh, *lshu, *lshv;   /* adjoint of the predictor state (scratch) */
+    float *uh, *ulo, *uhu, *uhv; /* the predictor state, recomputed (scratch) */
+    uint32_t *mark;             /* n_blocks: tag of the step whose active blocks these are (scratch) */
+    float *gn;                  /* d loss / d Manning n, per cell (accumulated) */
+    float *gz;                  /* d loss / d bed elevation, per cell (accumulated) */
+    double *gq;                 /* d loss / d knot discharge, per knot of swe_sources_t (accumulated) */
+} swe_adjoint_t;
+
+/* Gauges of the misfit (device pointers). */
+typedef struct {
+    const uint32_t *cells; /* distinct gauge cells */
+    float *obs;            /* steps x count: observed (h + h_lo) after each step */
+    double *loss;          /* the accumulated misfit */
+    uint32_t count;
+    uint32_t steps;
+} swe_gauges_t;
+
+/* Bed steps of every edge record from a bed z (n padded cells): face =
+   max(zL, zR) in float64, dzL = face - zL, dzR = face - zR, as the geometry
+   computes them (inundation/mesh/geometry.py:241-254). */
+int swe_bed_steps(const swe_mesh_t *mesh, const float *z, float *tile_dzl, float *tile_dzr, uint32_t tile_records,
+                  float *sub_dzl, float *sub_dzr, uint32_t sub_records, swe_stream_t stream);
+
+/* swe_stage with 256-cell blocks that also stores every computed cell's gathered sums. */
+int swe_stage_taped(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params_t *params, int stage,
+                    float *sums, swe_stream_t stream);
+
+/* Copies the state, dt, clock and active list at the start of a step into tape slot `slot`
+   (slot == capacity: the end state only). */
+int swe_tape_record(const swe_mesh_t *mesh, const swe_state_t *state, const swe_tape_t *tape, uint32_t slot,
+                    swe_stream_t stream);
+
+/* After a step: record == 1 writes (h + h_lo) at the gauges into obs row steps - 1 (the
+   control block's count of real steps); record == 0 adds the squared misfit against that row to *loss. */
+int swe_gauge_misfit(const swe_state_t *state, const swe_gauges_t *gauges, int record, swe_stream_t stream);
+
+/* Reverses tape slots `slots - 1` down to 0 (slot k is the step from tape state k to k + 1):
+   for each, adds the misfit's gradient at the state after the step (obs row row0 + k), then
+   takes the adjoint back through the sources, the corrector and the predictor, accumulating
+   gn, gz and gq. Block marks use tags tag0 + k + 1, which must not repeat within a run (give
+   each segment its own range, e.g. tag0 = its first step's index). */
+int swe_adjoint_segment(const swe_mesh_t *mesh, const swe_params_t *params, const swe_tape_t *tape,
+                        const swe_adjoint_t *adj, const swe_sources_t *sources, const swe_gauges_t *gauges,
+                        uint32_t slots, uint32_t row0, uint32_t tag0, swe_stream_t stream);
+
 /* Sum of (h + h_lo) * area in float64, in a fixed order: partials holds
    swe_volume_partials(n) doubles. The reference does this on the host
    (inundation/workflow.py:913-922). */

@@ -134,9 +134,13 @@ __device__ __forceinline__ void edge_words(const Phys &p, int cR, float nx, floa
 
 // ---------------------------------------------------------------------------
 // 256-cell blocks, plain loads: persistent CTAs stride over the active list.
+// sums != nullptr: also store every computed cell's gathered sums (sdh, sdhu,
+// sdhv at sums[i], sums[n + i], sums[2n + i], n = padded cells), the record
+// the adjoint reverses.
 // ---------------------------------------------------------------------------
 template <int STAGE, bool COMP, bool CLAMP>
-__global__ void __launch_bounds__(kThreads) stage_block_kernel(swe_mesh_t m, swe_state_t s, Phys p, float cfl) {
+__global__ void __launch_bounds__(kThreads)
+    stage_block_kernel(swe_mesh_t m, swe_state_t s, Phys p, float cfl, float *sums) {
     const uint32_t cap = (m.max_tile_edges + 3u) & ~3u;
     const TileSmem t = tile_smem(cap);
     __shared__ uint32_t red[kThreads / 32];
@@ -198,6 +202,12 @@ __global__ void __launch_bounds__(kThreads) stage_block_kernel(swe_mesh_t m, swe
             const float loi = COMP ? (STAGE ? s.h1_lo[i] : s.h_lo[i]) : 0.0f;
             const float h0 = STAGE ? s.h[i] : 0.0f, hu0 = STAGE ? s.hu[i] : 0.0f, hv0 = STAGE ? s.hv[i] : 0.0f;
             const float lo0 = (STAGE && COMP) ? s.h_lo[i] : 0.0f;
+            if (sums) {
+                const uint32_t n = m.n_blocks * kBlockCells;
+                sums[i] = sdh;
+                sums[n + i] = sdhu;
+                sums[2 * n + i] = sdhv;
+            }
             update_cell<STAGE, COMP, CLAMP>(s, p, cfl, dt, i, m.area[i], m.n_mann[i], hi, hui, hvi, loi, h0, hu0, hv0,
                                             lo0, sdh, sdhu, sdhv, lam, wet, bound);
         }
@@ -469,15 +479,16 @@ __global__ void __launch_bounds__(kTileThreads, 8) stage_tiled_kernel(swe_mesh_t
 // Host side.
 // ---------------------------------------------------------------------------
 template <int STAGE, bool COMP, bool CLAMP>
-int launch_stage(const swe_mesh_t *m, const swe_state_t *s, const swe_params_t *p, cudaStream_t st) {
+int launch_stage(const swe_mesh_t *m, const swe_state_t *s, const swe_params_t *p, cudaStream_t st,
+                 float *sums = nullptr) {
     const Phys ph{p->g, p->dry_tol};
-    if (p->kernel == 1u) {
+    if (p->kernel == 1u || sums) {
         auto kern = stage_block_kernel<STAGE, COMP, CLAMP>;
         const size_t bytes = block_smem_bytes(m->max_tile_edges);
         int rc = set_smem(kern, bytes);
         if (rc) return rc;
         const uint32_t grid = (p->grid == 0u || p->grid > m->n_blocks) ? m->n_blocks : p->grid;
-        kern<<<grid, kThreads, bytes, st>>>(*m, *s, ph, p->cfl);
+        kern<<<grid, kThreads, bytes, st>>>(*m, *s, ph, p->cfl, sums);
         return check_launch();
     }
     auto kern = stage_tiled_kernel<STAGE, COMP, CLAMP>;
@@ -489,11 +500,14 @@ int launch_stage(const swe_mesh_t *m, const swe_state_t *s, const swe_params_t *
 }
 
 template <int STAGE>
-int dispatch_stage(const swe_mesh_t *m, const swe_state_t *s, const swe_params_t *p, cudaStream_t st) {
+int dispatch_stage(const swe_mesh_t *m, const swe_state_t *s, const swe_params_t *p, cudaStream_t st,
+                   float *sums = nullptr) {
     if (p->compensated) {
-        return p->track_clamp ? launch_stage<STAGE, true, true>(m, s, p, st) : launch_stage<STAGE, true, false>(m, s, p, st);
+        return p->track_clamp ? launch_stage<STAGE, true, true>(m, s, p, st, sums)
+                              : launch_stage<STAGE, true, false>(m, s, p, st, sums);
     }
-    return p->track_clamp ? launch_stage<STAGE, false, true>(m, s, p, st) : launch_stage<STAGE, false, false>(m, s, p, st);
+    return p->track_clamp ? launch_stage<STAGE, false, true>(m, s, p, st, sums)
+                          : launch_stage<STAGE, false, false>(m, s, p, st, sums);
 }
 
 template <int STAGE, bool COMP, bool CLAMP>
@@ -537,6 +551,14 @@ int swe_stage(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params
     if (!mesh_ok(mesh) || !state_ok(state) || !params || params->kernel > 1u) return SWE_ERR_ARGUMENT;
     if (stage == 0) return dispatch_stage<0>(mesh, state, params, stream);
     if (stage == 1) return dispatch_stage<1>(mesh, state, params, stream);
+    return SWE_ERR_ARGUMENT;
+}
+
+int swe_stage_taped(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params_t *params, int stage,
+                    float *sums, swe_stream_t stream) {
+    if (!mesh_ok(mesh) || !state_ok(state) || !params || !sums) return SWE_ERR_ARGUMENT;
+    if (stage == 0) return dispatch_stage<0>(mesh, state, params, stream, sums);
+    if (stage == 1) return dispatch_stage<1>(mesh, state, params, stream, sums);
     return SWE_ERR_ARGUMENT;
 }
 

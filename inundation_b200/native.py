@@ -40,6 +40,11 @@ _SIGNATURES: dict[str, tuple[list, object]] = {
     "swe_eft_probe": ([_P, _P], ctypes.c_int),
     "swe_pow43": ([_P, _P, _U32, _P], ctypes.c_int),
     "swe_status_string": ([ctypes.c_int], ctypes.c_char_p),
+    "swe_bed_steps": ([_P, _P, _P, _P, _U32, _P, _P, _U32, _P], ctypes.c_int),
+    "swe_stage_taped": ([_P, _P, _P, ctypes.c_int, _P, _P], ctypes.c_int),
+    "swe_tape_record": ([_P, _P, _P, _U32, _P], ctypes.c_int),
+    "swe_gauge_misfit": ([_P, _P, ctypes.c_int, _P], ctypes.c_int),
+    "swe_adjoint_segment": ([_P, _P, _P, _P, _P, _P, _U32, _U32, _U32, _P], ctypes.c_int),
 }
 
 
@@ -91,6 +96,24 @@ class SweSources(ctypes.Structure):
         ("count", _U32),
         ("n_hydro", _U32),
     ]
+
+
+class SweTape(ctypes.Structure):
+    _fields_ = [
+        *[(name, _P) for name in ("h", "hu", "hv", "h_lo", "s0", "s1", "dt", "t", "list", "count")],
+        ("capacity", _U32),
+    ]
+
+
+class SweAdjoint(ctypes.Structure):
+    _fields_ = [
+        (name, _P)
+        for name in ("lh", "lhu", "lhv", "ls", "lsh", "lshu", "lshv", "uh", "ulo", "uhu", "uhv", "mark", "gn", "gz", "gq")
+    ]
+
+
+class SweGauges(ctypes.Structure):
+    _fields_ = [("cells", _P), ("obs", _P), ("loss", _P), ("count", _U32), ("steps", _U32)]
 
 
 _LIB: ctypes.CDLL | None = None

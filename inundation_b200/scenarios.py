@@ -12,6 +12,8 @@ name.
   3 m channel, 4 m of water inside 500 m of the centre, n = 0.035, 1 h.
 * ``rain_inflow``   -- 4M cells, 40 m relief, n log-uniform in [0.02, 0.08], 50 mm/h rain
   for 30 min and a triangular 200 m^3/s inflow peaking at 20 min, initially dry.
+* ``calibration``   -- the adjoint problem: a pond plus an inflow hydrograph of 32 knots,
+  200 gauges, a seeded "true" Manning field.
 * ``batch_member``  -- one of the batched scenarios: N cells, own DEM, n in
   [0.02, 0.06], triangular inflow of 10-300 m^3/s peaking at 20 min, initially dry.
 """
@@ -134,6 +136,38 @@ def batch_member(n_cells: int, seed: int, spacing: float = 10.0) -> Scenario:
     inflow = Hydrograph(cells=np.array([cell]), knot_t=kt, knot_q=kq)
     return Scenario("batch_member", geom, z.copy(), z.copy(), z.copy(), manning, t_end=1800.0, hydrographs=[inflow],
                     meta={"inflow_cell": cell, "peak_m3s": peak})
+
+
+def calibration(n_cells: int = 250_000, seed: int = 5, knots: int = 32, gauges: int = 200,
+                spacing: float = 10.0) -> Scenario:
+    """The adjoint workload: a pond on fractal terrain fed by an inflow hydrograph.
+
+    A Voronoi mesh at ``spacing`` m on a fractal DEM (beta 2, 20 m relief),
+    1 m of water within 10 % of the side of a centre point, a triangular
+    inflow there (200 m^3/s at 20 min, 0 at 30 min) given by ``knots``
+    evenly spaced knots over 30 min, ``gauges`` seeded cells within 20 % of
+    the side of that point, and a seeded "true" Manning field uniform in
+    [0.02, 0.06]; ``manning`` (the starting guess) is 0.035 everywhere.
+    """
+    side = spacing * np.sqrt(n_cells)
+    geom = voronoi_geometry(n_cells, side, seed)
+    geom = with_bed(geom, fractal_terrain(geom, side, 20.0, seed))
+    rng = np.random.default_rng(seed)
+    xy = geom.world_centroid
+    centre = np.array([0.4 * side, 0.5 * side])
+    r = np.hypot(xy[:, 0] - centre[0], xy[:, 1] - centre[1])
+    h0 = np.where(r <= 0.1 * side, 1.0, 0.0).astype(np.float32)
+    inflow_cell = int(np.argmin(r))
+    kt = np.linspace(0.0, 1800.0, knots).astype(np.float32)
+    kq = np.asarray(triangular_hydrograph(kt.astype(np.float64), 200.0, 1200.0, 1800.0), np.float32)
+    inflow = Hydrograph(cells=np.array([inflow_cell]), knot_t=kt, knot_q=kq)
+    near = np.flatnonzero(r <= 0.2 * side)
+    gauge_cells = np.sort(rng.choice(near, size=min(gauges, near.size), replace=False))
+    n_true = rng.uniform(0.02, 0.06, geom.N).astype(np.float32)
+    z = np.zeros(geom.N, np.float32)
+    return Scenario("calibration", geom, h0, z, z.copy(), np.full(geom.N, 0.035, np.float32), t_end=1800.0,
+                    hydrographs=[inflow],
+                    meta={"gauges": gauge_cells, "n_true": n_true, "inflow_cell": inflow_cell, "peak_m3s": 200.0})
 
 
 def batch_sizes(count: int = 64, lo: int = 20_000, hi: int = 500_000, seed: int = 4) -> list[int]:

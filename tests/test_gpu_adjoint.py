@@ -1,0 +1,180 @@
+"""The CUDA adjoint of the gauge misfit against float64 references.
+
+* the gradient with respect to Manning's n, the bed and the hydrograph knots
+  against float64 ``torch.autograd`` of the same discrete step (dt frozen at
+  the CUDA run's values), relative error per parameter group;
+* directional derivatives against float64 central finite differences of the
+  same float64 step on random directions (error relative to the summed size of
+  the n, z and q terms, which can cancel);
+* the adjoint of one and three steps from a wet float32 state, every cell a
+  gauge, against float64 autograd from the same state (1e-4): the per-step
+  adjoint is exact to float32 rounding, and what remains over many steps is
+  the float32 trajectory's drift from the float64 one;
+* the gradient does not depend on the checkpoint interval (bit for bit), and
+  ``MisfitFunction`` hands it to ``torch.autograd``.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from inundation_b200.scenarios import calibration
+from oracle.torch_step import TorchStep, misfit
+
+pytestmark = pytest.mark.gpu
+
+STEPS = 120
+REL_TOL = 1e-3
+
+
+@pytest.fixture(scope="module")
+def case():
+    from inundation_b200.adjoint import GaugeCalibration
+
+    sc = calibration(4000, seed=7, knots=8, gauges=40, spacing=10.0)
+    prob = GaugeCalibration(sc.geom, sc.h0, sc.hu0, sc.hv0, gauges=sc.meta["gauges"], steps=STEPS,
+                            hydrographs=sc.hydrographs, checkpoint_every=50, dt_max=1.0, dt_init=0.05)
+    z = sc.geom.zb.astype(np.float32)
+    q = sc.hydrographs[0].knot_q.astype(np.float32)
+    obs = prob.observe(sc.meta["n_true"], z, q)
+    n = sc.manning.copy()
+    loss = prob.loss(n, z, q)
+    gn, gz, gq = prob.gradient()
+    dts, ts = prob.clock()
+    return {"sc": sc, "prob": prob, "obs": obs, "n": n, "z": z, "q": q, "loss": loss, "grads": (gn, gz, gq),
+            "dts": dts, "ts": ts}
+
+
+def reference(c, n, z, q, grad: bool):
+    sc = c["sc"]
+    g = sc.geom
+    model = TorchStep(g, dry_tol=1e-4)
+    t64 = lambda a: torch.as_tensor(np.asarray(a, np.float64))  # noqa: E731
+    n_t, z_t, q_t = (t64(v).requires_grad_(grad) for v in (n, z, q))
+    hg = sc.hydrographs[0]
+    cells = torch.as_tensor(np.asarray(hg.cells, np.int64))
+    area = np.asarray(g.area, np.float32)
+    hscale = t64((hg.shares() * (1.0 / area[hg.cells]).astype(np.float32)).astype(np.float64))
+    hydro = [(cells, hscale, t64(hg.knot_t), slice(0, hg.knot_q.size))]
+    loss = misfit(model, t64(sc.h0), t64(sc.hu0), t64(sc.hv0), n_t, z_t, q_t, c["dts"], c["ts"],
+                  torch.as_tensor(np.asarray(sc.meta["gauges"], np.int64)), t64(c["obs"]), hydro=hydro,
+                  checkpoint=grad)
+    if not grad:
+        return float(loss)
+    loss.backward()
+    return float(loss.detach()), n_t.grad.numpy(), z_t.grad.numpy(), q_t.grad.numpy()
+
+
+def rel(a, b) -> float:
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def test_clock_runs_every_step_and_the_loss_is_positive(case) -> None:
+    assert case["dts"].size == STEPS and (case["dts"] > 0).all()
+    assert case["loss"] > 0.0
+
+
+def test_gradient_matches_float64_autograd(case) -> None:
+    loss64, gn64, gz64, gq64 = reference(case, case["n"], case["z"], case["q"], grad=True)
+    assert case["loss"] == pytest.approx(loss64, rel=1e-3)
+    gn, gz, gq = case["grads"]
+    errs = {"n": rel(gn, gn64), "z": rel(gz, gz64), "q": rel(gq, gq64)}
+    assert all(np.linalg.norm(v) > 0 for v in (gn64, gz64, gq64))
+    assert max(errs.values()) <= REL_TOL, errs
+
+
+def central_difference(case, dn, dz, dq, eps: float) -> float:
+    n0, z0, q0 = (case[k].astype(np.float64) for k in ("n", "z", "q"))
+    plus = reference(case, n0 + eps * dn, z0 + eps * dz, q0 + eps * dq, grad=False)
+    minus = reference(case, n0 - eps * dn, z0 - eps * dz, q0 - eps * dq, grad=False)
+    return (plus - minus) / (2 * eps)
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_directional_derivatives_match_float64_finite_differences(case, seed: int) -> None:
+    """A direction counts only where two step sizes agree: a perturbation that moves a cell
+    across a dry threshold or a flux region makes the loss jump, and no derivative sees that."""
+    gn, gz, gq = case["grads"]
+    tries = []
+    for attempt in range(3):
+        rng = np.random.default_rng(100 + 10 * seed + attempt)
+        dn = rng.standard_normal(case["n"].size) * 0.005
+        dz = rng.standard_normal(case["z"].size) * 0.01
+        dq = rng.standard_normal(case["q"].size) * 2.0
+        fd = central_difference(case, dn, dz, dq, 1e-5)
+        fd_fine = central_difference(case, dn, dz, dq, 2e-6)
+        tries.append((fd, fd_fine))
+        if abs(fd - fd_fine) <= 1e-4 * abs(fd):
+            break
+    else:
+        pytest.fail(f"no smooth direction in three tries: {tries}")
+    parts = (float(np.dot(gn, dn)), float(np.dot(gz, dz)), float(np.dot(gq, dq)))
+    ad = sum(parts)
+    # Relative to the size of the three groups' terms: they can cancel, and a relative error
+    # of the sum would then magnify the float32 trajectory's drift from the float64 one.
+    scale = sum(abs(v) for v in parts)
+    assert abs(ad - fd) <= REL_TOL * scale, (ad, fd, parts, attempt)
+
+
+def test_gradient_does_not_depend_on_the_checkpoint_interval(case) -> None:
+    from inundation_b200.adjoint import GaugeCalibration
+
+    sc = case["sc"]
+    other = GaugeCalibration(sc.geom, sc.h0, sc.hu0, sc.hv0, gauges=sc.meta["gauges"], steps=STEPS,
+                             hydrographs=sc.hydrographs, checkpoint_every=7, dt_max=1.0, dt_init=0.05)
+    other.set_observations(case["obs"])
+    assert other.loss(case["n"], case["z"], case["q"]) == case["loss"]
+    for a, b in zip(other.gradient(), case["grads"], strict=True):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_misfit_function_feeds_torch_autograd(case) -> None:
+    from inundation_b200.adjoint import MisfitFunction
+
+    prob = case["prob"]
+    dev = prob.device
+    n = torch.tensor(case["n"], device=dev, requires_grad=True)
+    z = torch.tensor(case["z"], device=dev, requires_grad=True)
+    q = torch.tensor(case["q"], device=dev, requires_grad=True)
+    loss = MisfitFunction.apply(n, z, q, prob)
+    (3.0 * loss).backward()
+    assert float(loss.detach()) == case["loss"]
+    gn, gz, gq = case["grads"]
+    np.testing.assert_allclose(n.grad.cpu().numpy(), 3.0 * gn, rtol=1e-6)
+    np.testing.assert_allclose(z.grad.cpu().numpy(), 3.0 * gz, rtol=1e-6)
+    np.testing.assert_allclose(q.grad.cpu().numpy(), 3.0 * gq, rtol=1e-6)
+
+
+@pytest.mark.parametrize("steps", [1, 3])
+def test_few_step_adjoint_matches_float64_autograd_from_a_wet_state(case, steps: int) -> None:
+    """Every cell a gauge with a random observation, from a state in the middle of a run with
+    wetting fronts: the adjoint of one to three steps against float64 autograd from the same
+    float32 state (trajectories can only drift apart by a few steps' rounding)."""
+    from inundation_b200.adjoint import GaugeCalibration
+
+    sc, prob = case["sc"], case["prob"]
+    mid = GaugeCalibration(sc.geom, sc.h0, sc.hu0, sc.hv0, gauges=sc.meta["gauges"], steps=60,
+                           hydrographs=sc.hydrographs, checkpoint_every=60, dt_max=1.0, dt_init=0.05)
+    mid.loss(case["n"], case["z"], case["q"], checkpoints=False)
+    h, hu, hv = (mid.download_state(k) for k in ("h", "hu", "hv"))
+    assert (h >= 1e-4).sum() > 100
+    rng = np.random.default_rng(steps)
+    all_cells = np.arange(sc.geom.N)
+    p = GaugeCalibration(sc.geom, h, hu, hv, gauges=all_cells, steps=steps, hydrographs=sc.hydrographs,
+                         checkpoint_every=2, dt_max=1.0, dt_init=0.05)
+    obs = (np.repeat(h[None, :], steps, 0) + rng.normal(0.0, 0.01, (steps, sc.geom.N))).astype(np.float32)
+    p.set_observations(obs)
+    p.loss(case["n"], case["z"], case["q"])
+    gn, gz, gq = p.gradient()
+    dts, ts = p.clock()
+    c = {"sc": sc, "dts": dts, "ts": ts, "obs": obs}
+    saved = (sc.h0, sc.hu0, sc.hv0, sc.meta["gauges"])
+    sc.h0, sc.hu0, sc.hv0, sc.meta["gauges"] = h, hu, hv, all_cells
+    try:
+        _, gn64, gz64, gq64 = reference(c, case["n"], case["z"], case["q"], grad=True)
+    finally:
+        sc.h0, sc.hu0, sc.hv0, sc.meta["gauges"] = saved
+    errs = {"n": rel(gn, gn64), "z": rel(gz, gz64), "q": rel(gq, gq64) if np.linalg.norm(gq64) > 0 else 0.0}
+    assert max(errs.values()) <= 1e-4, errs
