@@ -64,6 +64,9 @@ def parse_args() -> argparse.Namespace:
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-scenarios measurement")
     ap.add_argument("--batch-count", type=int, default=64, help="scenarios in the batched measurement")
     ap.add_argument("--batch-steps", type=int, default=2000, help="steps of every scenario in the batched measurement")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the forward+adjoint measurement")
+    ap.add_argument("--adjoint-cells", type=int, default=250_000)
+    ap.add_argument("--adjoint-steps", type=int, default=2000)
     return ap.parse_args()
 
 
@@ -407,6 +410,8 @@ def run_b200(args, world: int, rank: int, local: int) -> None:
     torch.cuda.empty_cache()
     if not args.no_batch:
         line["batched"] = run_batch(args, world, local)
+    if not args.no_adjoint:
+        line["adjoint"] = run_adjoint(args, world, local)
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -589,6 +594,125 @@ def run_batch(args, world: int, local: int) -> dict:
         "gpu_launches": launches_per_step * steps,
         "clocks": clock,
     }
+
+
+# -- forward + adjoint --------------------------------------------------------------------------------
+def _adjoint_problem(cells: int, steps: int, knots: int, gauges: int, device: str, seed: int = 5,
+                     checkpoint_every: int = 50):
+    from inundation_b200.adjoint import GaugeCalibration
+    from inundation_b200.scenarios import calibration
+
+    sc = calibration(cells, seed=seed, knots=knots, gauges=gauges)
+    prob = GaugeCalibration(sc.geom, sc.h0, sc.hu0, sc.hv0, gauges=sc.meta["gauges"], steps=steps,
+                            hydrographs=sc.hydrographs, checkpoint_every=checkpoint_every, dt_max=sc.dt_max,
+                            dt_init=sc.dt_init, device=device)
+    prob.cut_depth = 4.0 * sc.dry_tol
+    z = sc.geom.zb.astype(np.float32)
+    q = sc.hydrographs[0].knot_q.astype(np.float32)
+    prob.observe(sc.meta["n_true"], z, q)
+    return sc, prob, sc.manning.copy(), z, q
+
+
+def _gradient_error(device: str) -> dict:
+    """The CUDA gradient against float64 torch autograd of the same discrete step (dt frozen, the
+    same film-depth cut), on a 4000-cell instance of the calibration problem over 120 steps. Each
+    model is compared on its own observations (the float64 reference recomputes the gauge depths
+    of the "true" run with that run's clock), so residuals share each model's rounding. The
+    float64 reference runs on the host CPU."""
+    import torch
+
+    from oracle.torch_step import TorchStep, hydrograph_value, misfit
+
+    sc, prob, n, z, q = _adjoint_problem(4000, 120, 8, 40, device, seed=7)
+    true_dts, true_ts = prob.clock()
+    loss32 = prob.loss(n, z, q)
+    gn, gz, gq = prob.gradient()
+    dts, ts = prob.clock()
+    g = sc.geom
+    model = TorchStep(g, dry_tol=sc.dry_tol, cut_depth=prob.cut_depth)
+    t64 = lambda a: torch.as_tensor(np.asarray(a, np.float64))  # noqa: E731
+    hg = sc.hydrographs[0]
+    cells = torch.as_tensor(np.asarray(hg.cells, np.int64))
+    hscale = t64((hg.shares() * (1.0 / np.asarray(g.area, np.float32)[hg.cells]).astype(np.float32)).astype(np.float64))
+    gauges = torch.as_tensor(np.asarray(sc.meta["gauges"], np.int64))
+    obs = []
+    with torch.no_grad():
+        dzL, dzR = model.bed_steps(t64(z))
+        h, hu, hv = t64(sc.h0), t64(sc.hu0), t64(sc.hv0)
+        for dt, t in zip(true_dts, true_ts, strict=True):
+            h, hu, hv = model.step(h, hu, hv, t64(sc.meta["n_true"]), dzL, dzR, dt, cells,
+                                   hscale * hydrograph_value(t64(hg.knot_t), t64(q), t))
+            obs.append(h[gauges].numpy().copy())
+    n_t, z_t, q_t = (t64(v).requires_grad_(True) for v in (n, z, q))
+    loss = misfit(model, t64(sc.h0), t64(sc.hu0), t64(sc.hv0), n_t, z_t, q_t, dts, ts, gauges, t64(np.array(obs)),
+                  hydro=[(cells, hscale, t64(hg.knot_t), slice(0, hg.knot_q.size))])
+    loss.backward()
+    rel = lambda a, b: float(np.linalg.norm(a.astype(np.float64) - b) / np.linalg.norm(b))  # noqa: E731
+    return {
+        "reference": "float64 torch autograd of the same discrete step, dt frozen, same film-depth cut; "
+        "4000 cells, 120 steps, 8 knots, 40 gauges",
+        "loss_rel": abs(loss32 - float(loss.detach())) / float(loss.detach()),
+        "grad_rel_n": rel(gn, n_t.grad.numpy()),
+        "grad_rel_z": rel(gz, z_t.grad.numpy()),
+        "grad_rel_q": rel(gq, q_t.grad.numpy()),
+        "tolerance": 1e-3,
+    }
+
+
+def run_adjoint(args, world: int, local: int) -> dict:
+    """Forward and forward+adjoint of the calibration problem, device time of each.
+
+    A seeded 250k-cell Voronoi mesh (10 m spacing) on a fractal DEM, a 1 m pond and a
+    triangular inflow hydrograph of 32 knots, 200 gauges, 2000 steps; the misfit against a run
+    with a seeded Manning field, its gradient with respect to n, bed and knots with a
+    checkpoint every 50 steps.
+    """
+    import torch
+
+    device = f"cuda:{local}"
+    sc, prob, n, z, q = _adjoint_problem(args.adjoint_cells, args.adjoint_steps, 32, 200, device)
+    prob.loss(n, z, q)  # capture the graphs and warm up
+    prob.backward()
+    prob.set_parameters(n, z, q)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    torch.cuda.synchronize()
+    ev[0].record(prob._stream)
+    prob._run(record=0, checkpoints=False)
+    ev[1].record(prob._stream)
+    ev[1].synchronize()
+    ev[2].record(prob._stream)
+    prob._run(record=0, checkpoints=True)
+    prob._has_forward = True
+    prob.backward()
+    ev[3].record(prob._stream)
+    ev[3].synchronize()
+    fwd_ms = ev[0].elapsed_time(ev[1])
+    both_ms = ev[2].elapsed_time(ev[3])
+    gn, gz, gq = prob.gradient()
+    cells, steps = int(sc.geom.N), prob.steps
+    out = {
+        "workload": f"calibration_{cells // 1000}k_voronoi",
+        "cells": cells,
+        "steps": steps,
+        "gauges": int(prob.gauges.size),
+        "knots": prob.n_knots,
+        "checkpoint_every": prob.K,
+        "fwd_ms": fwd_ms,
+        "fwd_adj_ms": both_ms,
+        "fwd_cell_steps_per_s": cells * steps / (fwd_ms * 1e-3),
+        "fwd_adj_cell_steps_per_s": cells * steps / (both_ms * 1e-3),
+        "ratio_fwd_adj_over_fwd": both_ms / fwd_ms,
+        "target_ratio": 4.0,
+        "grad_norms": {"n": float(np.linalg.norm(gn)), "z": float(np.linalg.norm(gz)), "q": float(np.linalg.norm(gq))},
+        "grad_finite": bool(np.isfinite(gn).all() and np.isfinite(gz).all() and np.isfinite(gq).all()),
+        "cut_depth_m": prob.cut_depth,
+        "note": "fwd = the misfit run alone; fwd+adj = the run with checkpoints, then every segment taped "
+        "again and reversed",
+    }
+    del prob
+    torch.cuda.empty_cache()
+    out["gradient_error"] = _gradient_error(device)
+    return out
 
 
 # -- reference arm ---------------------------------------------------------------------------------

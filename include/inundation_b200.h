@@ -236,6 +236,8 @@ typedef struct {
     float *gn;                  /* d loss / d Manning n, per cell (accumulated) */
     float *gz;                  /* d loss / d bed elevation, per cell (accumulated) */
     double *gq;                 /* d loss / d knot discharge, per knot of swe_sources_t (accumulated) */
+    float cut_depth;            /* no derivative flows through a cell or face depth below this (0: the
+                                   exact derivative of the discrete step) */
 } swe_adjoint_t;
 
 /* Gauges of the misfit (device pointers). */

@@ -48,7 +48,18 @@ def _as_tensor(x, device, dtype=torch.float32) -> torch.Tensor:
 
 
 class GaugeCalibration(ResidentEngine):
-    """Misfit of ``steps`` resident steps at gauge cells, and its adjoint gradient."""
+    """Misfit of ``steps`` resident steps at gauge cells, and its adjoint gradient.
+
+    ``cut_depth`` (metres, 0 by default): no derivative flows through a cell
+    depth or a face depth below it. 0 gives the exact derivative of the
+    discrete step. Over long runs with wetting fronts that derivative is
+    dominated by cells near the dry threshold (film drag, the desingularised
+    velocity and the dry-bed wave-speed blend change steeply there) and can
+    grow without bound; a cut at the film depth (4 dry_tol) keeps the
+    derivatives of the wet flow only.
+    """
+
+    cut_depth: float = 0.0
 
     def __init__(
         self,
@@ -316,6 +327,7 @@ class GaugeCalibration(ResidentEngine):
             raise RuntimeError("call loss(...) with checkpoints before the gradient")
         params, sources = self._params(), self._sources()
         params.grid = min(self.n_blocks, 4 * self._sms)
+        self._adj.cut_depth = float(self.cut_depth)
         with torch.cuda.stream(self._stream):
             for t in self._adj_t.values():
                 t.zero_()

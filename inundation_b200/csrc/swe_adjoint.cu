@@ -92,41 +92,44 @@ __device__ __forceinline__ CellFwd cell_forward(const Phys &p, float dt, float A
 // to the adjoints of the inputs (state, sums) and of n.
 __device__ __forceinline__ void cell_reverse(const Phys &p, float dt, float A, float n, const CellFwd &c, float gH,
                                              float gHU, float gHV, float &g_h, float &g_hu, float &g_hv, float &g_sdh,
-                                             float &g_sdhu, float &g_sdhv, float &g_n) {
+                                             float &g_sdhu, float &g_sdhv, float &g_n, bool cut_in, float cut) {
     const float dti = dt / A;
     float g_hua = 0.0f, g_hva = 0.0f;
     if (c.wet) {
         const float h = c.h_new;
+        const bool thin = h < cut;  // friction and drag depth held constant
         float g_hub = gHU / c.den, g_hvb = gHV / c.den;
         const float g_den = -(gHU * c.hu_new + gHV * c.hv_new) / c.den;
         const float g_Sf = g_den * dt;
         g_n += g_Sf * 2.0f * p.g * n * c.spd / c.P;
         const float g_spd = g_Sf * p.g * n * n / c.P;
         const float g_P = -g_Sf * c.Sf / c.P;
-        gH += g_P * (4.0f / 3.0f) * c.P / h;
+        if (!thin) gH += g_P * (4.0f / 3.0f) * c.P / h;
         if (c.spd > 0.0f) {
             const float g_u = g_spd * c.u / c.spd, g_v = g_spd * c.v / c.spd;
             g_hub += g_u / h;
             g_hvb += g_v / h;
-            gH -= (g_u * c.u + g_v * c.v) / h;
+            if (!thin) gH -= (g_u * c.u + g_v * c.v) / h;
         }
         g_hua = g_hub * c.drag;
         g_hva = g_hvb * c.drag;
         const float e = kFilmDepths * p.dry_tol;
-        if (h < e) {
+        if (h < e && !thin) {
             // drag = 1 / (1 + dt rate), rate = (e^2 - h^2) / (2 h^2) sqrt(g / e): d drag / dh = dt e^2 / h^3 sqrt(g/e) drag^2
             const float g_drag = g_hub * c.hu_a + g_hvb * c.hv_a;
             gH += g_drag * dt * e * e / (h * h * h) * sqrtf(p.g / e) * c.drag * c.drag;
         }
     }
     if (!c.clamped) {
-        g_h += gH;
+        if (!cut_in) g_h += gH;
         g_sdh = -dti * gH;
     } else {
         g_sdh = 0.0f;
     }
-    g_hu += g_hua;
-    g_hv += g_hva;
+    if (!cut_in) {
+        g_hu += g_hua;
+        g_hv += g_hva;
+    }
     g_sdhu = -dti * g_hua;
     g_sdhv = -dti * g_hva;
 }
@@ -156,7 +159,7 @@ struct EdgeGrad {
 // the forward's expressions, so every branch is the one the forward took.
 __device__ EdgeGrad edge_words_rev(const Phys &p, bool wall, float nx, float ny, float len, float dzL, float dzR,
                                    float hL, float huL, float hvL, float hR, float huR, float hvR, float g0, float g1,
-                                   float g2, float g3, float g4) {
+                                   float g2, float g3, float g4, float cut) {
     // ---- primal (face_states, hllc_speeds_fast, hllc) ----
     const float hLs = gmax(0.0f, hL - dzL);
     const float hRs = gmax(0.0f, hR - dzR);
@@ -320,13 +323,18 @@ __device__ EdgeGrad edge_words_rev(const Phys &p, bool wall, float nx, float ny,
     safe_vel_rev(p, hR, huR, ghuRs * hRs, G.hR, G.huR);
     safe_vel_rev(p, hR, hvR, ghvRs * hRs, G.hR, G.hvR);
     // hydrostatic reconstruction h* = max(0, h - dz)
-    if (0.0f < hL - dzL) {
+    if (0.0f < hL - dzL && !(hLs < cut)) {
         G.hL += ghLs;
         G.dzL = -ghLs;
     }
-    if (0.0f < hR - dzR) {
+    if (0.0f < hR - dzR && !(hRs < cut)) {
         G.hR += ghRs;
         G.dzR = -ghRs;
+    }
+    if (hR < cut) G.hR = G.huR = G.hvR = G.dzR = 0.0f;
+    if (hL < cut) {
+        G.hL = G.huL = G.hvL = G.dzL = 0.0f;
+        if (wall) G.hR = G.huR = G.hvR = G.dzR = 0.0f;  // the ghost is the (held) left state
     }
     if (wall) {
         // the ghost is the left state mirrored; a wall's bed steps are fixed at zero
@@ -428,7 +436,8 @@ __global__ void __launch_bounds__(kThreads)
         const float mom = (hf < p.dry_tol) ? 0.0f : 1.0f;
         const float gH = a.lh[i], gHU = a.lhu[i] * mom, gHV = a.lhv[i] * mom;
         float g_h = 0.0f, g_hu = 0.0f, g_hv = 0.0f, g_sh, g_su, g_sv, g_n = 0.0f;
-        cell_reverse(p, dt, A, nm, c1, 0.5f * gH, 0.5f * gHU, 0.5f * gHV, g_h, g_hu, g_hv, g_sh, g_su, g_sv, g_n);
+        cell_reverse(p, dt, A, nm, c1, 0.5f * gH, 0.5f * gHU, 0.5f * gHV, g_h, g_hu, g_hv, g_sh, g_su, g_sv, g_n,
+                     c0.h_new < a.cut_depth, a.cut_depth);
         a.ls[i] = g_sh;
         a.ls[n + i] = g_su;
         a.ls[2 * n + i] = g_sv;
@@ -457,7 +466,8 @@ __global__ void __launch_bounds__(kThreads)
         const CellFwd c0 =
             cell_forward(p, dt, A, nm, S.h[i], S.lo[i], S.hu[i], S.hv[i], S.s0[i], S.s0[n + i], S.s0[2 * n + i]);
         float g_h = 0.0f, g_hu = 0.0f, g_hv = 0.0f, g_sh, g_su, g_sv, g_n = 0.0f;
-        cell_reverse(p, dt, A, nm, c0, a.lsh[i], a.lshu[i], a.lshv[i], g_h, g_hu, g_hv, g_sh, g_su, g_sv, g_n);
+        cell_reverse(p, dt, A, nm, c0, a.lsh[i], a.lshu[i], a.lshv[i], g_h, g_hu, g_hv, g_sh, g_su, g_sv, g_n,
+                     S.h[i] < a.cut_depth, a.cut_depth);
         a.ls[i] = g_sh;
         a.ls[n + i] = g_su;
         a.ls[2 * n + i] = g_sv;
@@ -522,7 +532,7 @@ __global__ void __launch_bounds__(kThreads)
                 const float lhR = actR ? a.ls[cR] : 0.0f, luR = actR ? a.ls[n + cR] : 0.0f,
                             lvR = actR ? a.ls[2 * n + cR] : 0.0f;
                 eg = edge_words_rev(p, cR < 0, nx, ny, m.tile_len[e], m.tile_dzl[e], m.tile_dzr[e], hL, huL, hvL, hR,
-                                    huR, hvR, lhL - lhR, luL, lvL, -luR, -lvR);
+                                    huR, hvR, lhL - lhR, luL, lvL, -luR, -lvR, a.cut_depth);
             }
             const bool face_left = m.tile_dzl[e] == 0.0f;  // the face sits on the left bed
             G[j] = eg.hL;

@@ -41,10 +41,11 @@ def _div0(num: torch.Tensor, den: torch.Tensor, ok: torch.Tensor) -> torch.Tenso
 class TorchStep:
     """The discrete step over one mesh, float64, on ``device``."""
 
-    def __init__(self, geom, g: float = 9.81, dry_tol: float = 1e-4, device: str = "cpu") -> None:
+    def __init__(self, geom, g: float = 9.81, dry_tol: float = 1e-4, device: str = "cpu", cut_depth: float = 0.0) -> None:
         t = lambda a, dt=torch.float64: torch.as_tensor(np.asarray(a), dtype=dt, device=device)  # noqa: E731
         self.N, self.E = int(geom.N), int(geom.E)
         self.g, self.dry = float(g), float(dry_tol)
+        self.cut = float(cut_depth)  # no derivative through depths below this (0: the exact derivative)
         self.device = device
         self.cl = t(geom.edge_cellL, torch.int64)
         cr = np.asarray(geom.edge_cellR, np.int64)
@@ -61,17 +62,27 @@ class TorchStep:
         return torch.where(h > self.dry, 2.0 * h * q / (h2 + torch.maximum(h2, torch.full_like(h2, e2))),
                            torch.zeros_like(h))
 
+    def _cut(self, h, *vals):
+        if self.cut <= 0.0:
+            return vals
+        thin = h < self.cut
+        return tuple(torch.where(thin, v.detach(), v) for v in vals)
+
     def edge_words(self, h, hu, hv, dzL, dzR):
         g, dry = self.g, self.dry
         nx, ny, ln = self.nx, self.ny, self.len
         hL, huL, hvL = h[self.cl], hu[self.cl], hv[self.cl]
+        hL, huL, hvL = self._cut(hL, hL, huL, hvL)
         hR = torch.where(self.wall, hL, h[self.cr])
         dot = huL * nx + hvL * ny
         huR = torch.where(self.wall, huL - 2.0 * dot * nx, hu[self.cr])
         hvR = torch.where(self.wall, hvL - 2.0 * dot * ny, hv[self.cr])
+        hR, huR, hvR = self._cut(hR, hR, huR, hvR)
         zero = torch.zeros_like(hL)
         hLs = torch.clamp(hL - dzL, min=0.0)
         hRs = torch.clamp(hR - dzR, min=0.0)
+        (hLs,) = self._cut(hLs, hLs)
+        (hRs,) = self._cut(hRs, hRs)
         uL, vL, uR, vR = self._sv(hL, huL), self._sv(hL, hvL), self._sv(hR, huR), self._sv(hR, hvR)
         huLs, hvLs, huRs, hvRs = hLs * uL, hLs * vL, hRs * uR, hRs * vR
         hqnL, hqtL = huLs * nx + hvLs * ny, -huLs * ny + hvLs * nx
@@ -152,6 +163,7 @@ class TorchStep:
         g, dry = self.g, self.dry
         e = FILM_DEPTHS * dry
         dti = dt / self.area
+        h, hu, hv = self._cut(h, h, hu, hv)
         h_new = torch.clamp(h - dti * sh, min=0.0)
         hu_a = hu - dti * su
         hv_a = hv - dti * sv
@@ -159,10 +171,12 @@ class TorchStep:
         hs = torch.where(wet, h_new, torch.ones_like(h_new))
         rate = (e * e - hs * hs) / (2.0 * hs * hs) * np.sqrt(g / e)
         drag = torch.where(hs < e, 1.0 / (1.0 + dt * rate), torch.ones_like(hs))
+        (drag,) = self._cut(hs, drag)
         hu_b, hv_b = hu_a * drag, hv_a * drag
-        u, v = hu_b / hs, hv_b / hs
+        (hf,) = self._cut(hs, hs)  # the friction's depth
+        u, v = hu_b / hf, hv_b / hf
         spd = _sqrt0(u * u + v * v)
-        Sf = g * n * n * spd / torch.pow(hs, 4.0 / 3.0)
+        Sf = g * n * n * spd / torch.pow(hf, 4.0 / 3.0)
         den = 1.0 + dt * Sf
         hu_new = torch.where(wet, hu_b / den, torch.zeros_like(hu_b))
         hv_new = torch.where(wet, hv_b / den, torch.zeros_like(hv_b))
