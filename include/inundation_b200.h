@@ -47,7 +47,8 @@ typedef struct {
     uint32_t dry_dt_ticks;
     float last_raw;
     float cfl_safety;
-    uint32_t error;  /* set by the device: 1 = a bounded wait for staged data timed out */
+    uint32_t error;  /* set by the device: 1 = a bounded wait for staged data timed out,
+                        2 = a grid barrier of the persistent kernel timed out */
 } swe_ctrl_t;
 
 /* Static mesh in two tile layouts (device pointers).
@@ -115,6 +116,7 @@ typedef struct {
     uint32_t *dt_buf;              /* 4 words per instance: [0] this step's dt (float bits, 0 = no-op),
                                       [1] the next step's CFL bound */
     swe_ctrl_t *ctrl;              /* one per instance */
+    uint32_t *sync;                /* 64 zeroed words: the grid barrier of the persistent kernel (kernel 2) */
 } swe_state_t;
 
 typedef struct {
@@ -126,7 +128,9 @@ typedef struct {
     uint32_t active_set;  /* skip blocks outside the two-ring of wet blocks */
     uint32_t grid;        /* CTAs of the persistent stage kernels (0 = a default) */
     uint32_t kernel;      /* stage kernel: 0 = 64-cell tiles staged by bulk copies (default),
-                             1 = 256-cell blocks with plain loads */
+                             1 = 256-cell blocks with plain loads,
+                             2 = swe_steps only: whole steps of 64-cell tiles in one persistent cooperative
+                                 launch, phases separated by bounded grid barriers */
 } swe_params_t;
 
 /* Sparse sources (device pointers), one per cell: source k adds
@@ -147,6 +151,12 @@ typedef struct {
     uint32_t count;
     uint32_t n_hydro;
 } swe_sources_t;
+
+/* n_steps whole steps: swe_step n_steps times (kernel 0 or 1), or one persistent cooperative launch
+   running them all (kernel 2; params->grid caps its CTAs, 0 = as many as fit). A wait of the
+   persistent kernel that times out records error 2 in the control block. */
+int swe_steps(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params_t *params,
+              const swe_sources_t *sources, uint32_t n_steps, swe_stream_t stream);
 
 /* Bytes of device workspace of a mesh of n_blocks blocks and n_inst
    instances: active list, work items, sched words, dt words and control

@@ -1,0 +1,248 @@
+// Whole steps in one persistent, cooperative launch.
+//
+// The same phases as the per-kernel step (swe_step: predictor, corrector,
+// sources, dilation + step control) run back to back inside one kernel,
+// separated by grid-wide barriers instead of kernel boundaries, for
+// `n_steps` steps. A step with a few active tiles is a chain of short
+// dependent phases; between kernels each link pays a launch gap and a grid
+// ramp, between barriers about a microsecond.
+//
+// Every CTA is resident (cooperative launch), every barrier wait is bounded
+// (2 s, then the CTA records error 2 in the control block and stops), and the
+// staged-data waits of the tile passes are bounded as in the stage kernels.
+// The arithmetic is the stage kernels' own, so results are bit-identical.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "swe_sources.cuh"
+#include "swe_tiled.cuh"
+
+namespace swe {
+
+__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t *p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Generic-proxy writes of this phase before bulk-copy (async-proxy) reads of the next.
+__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
+
+struct GridSync {
+    uint32_t *count;  // arrivals of the current barrier
+    uint32_t *gen;    // barriers completed
+    uint32_t epoch;   // this CTA's view of gen (thread 0)
+};
+
+// Grid-wide barrier. The last CTA to arrive runs `last` (all its threads)
+// before it releases the others. False when this CTA's wait timed out.
+template <typename F>
+__device__ __forceinline__ bool grid_sync(GridSync &g, int *flag, F last) {
+    fence_proxy_async_global();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        flag[0] = (atomicAdd(g.count, 1u) == gridDim.x - 1) ? 1 : 0;
+        flag[1] = 1;
+    }
+    __syncthreads();
+    if (flag[0]) {
+        __threadfence();
+        last();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            atomicExch(g.count, 0u);
+            __threadfence();
+            atomicAdd(g.gen, 1u);
+        }
+    } else if (threadIdx.x == 0) {
+        const uint64_t t0 = global_ns();
+        while (ld_acquire_u32(g.gen) == g.epoch) {
+            if (global_ns() - t0 > kWaitLimitNs) {
+                flag[1] = 0;
+                break;
+            }
+        }
+        __threadfence();
+    }
+    g.epoch += 1u;
+    __syncthreads();
+    const bool ok = flag[1] != 0;
+    fence_proxy_async_global();
+    return ok;
+}
+
+// Dilation of the wet marks over each block's two-ring and compaction into the
+// next step's block list and tile work items (the dilate_compact kernel's work):
+// one lane per block, 32 blocks per warp, one pair of atomics per warp.
+__device__ __forceinline__ void dilate_pass(const swe_mesh_t &m, const swe_state_t &s, int all_active) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t chunk = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); chunk * 32u < m.n_blocks;
+         chunk += warps) {
+        const uint32_t b = chunk * 32u + lane;
+        uint32_t v = 0u;
+        if (b < m.n_blocks && s.dt_buf[kDtWords * m.block_inst[b]] != 0u) {
+            if (all_active) {
+                v = 1u;
+            } else {
+                v = s.blk[kBlkWords * b + kBlkWet] | s.blk[kBlkWords * b + kBlkForced];
+                for (uint32_t k = m.ring_ptr[b], k1 = m.ring_ptr[b + 1]; k < k1 && v == 0u; ++k) {
+                    const uint32_t nb = m.ring_idx[k];
+                    v = s.blk[kBlkWords * nb + kBlkWet] | s.blk[kBlkWords * nb + kBlkForced];
+                }
+                v = v ? 1u : 0u;
+            }
+            s.blk[kBlkWords * b + kBlkActive] = v;
+        }
+        const bool on = v != 0u;
+        const uint32_t cells = on ? m.block_cells[b] : 0u;
+        const uint32_t n_items = (cells + kTileCells - 1) / kTileCells;
+        const unsigned ballot = __ballot_sync(0xFFFFFFFFu, on);
+        uint32_t before = n_items;
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t up = __shfl_up_sync(0xFFFFFFFFu, before, d);
+            if (static_cast<int>(lane) >= d) before += up;
+        }
+        const uint32_t total = __shfl_sync(0xFFFFFFFFu, before, 31);
+        before -= n_items;
+        uint32_t pos = 0, ipos = 0;
+        if (lane == 0 && ballot) {
+            pos = atomicAdd(&s.sched[kSchedNext], static_cast<uint32_t>(__popc(ballot)));
+            ipos = atomicAdd(&s.sched[kSchedNextItems], total);
+        }
+        pos = __shfl_sync(0xFFFFFFFFu, pos, 0);
+        ipos = __shfl_sync(0xFFFFFFFFu, ipos, 0) + before;
+        if (on) {
+            const uint32_t slot = pos + __popc(ballot & ((1u << lane) - 1u));
+            if (slot < m.n_blocks) s.active_list[slot] = b;
+            const uint32_t inst = m.block_inst[b];
+            uint4 *out = reinterpret_cast<uint4 *>(s.items);
+            for (uint32_t q = 0; q < n_items && ipos + q < 4u * m.n_blocks; ++q) {
+                const uint32_t t = 4u * b + q;
+                const uint32_t l0 = m.sub_lcsr_ptr[t];
+                out[ipos + q] = make_item(t, min(static_cast<uint32_t>(kTileCells), cells - q * kTileCells),
+                                          m.sub_ptr[t], l0, m.sub_count[t], m.sub_lcsr_ptr[t + 1] - l0, inst);
+            }
+        }
+    }
+}
+
+template <bool COMP, bool CLAMP>
+__global__ void __launch_bounds__(kTileThreads)
+    persistent_steps_kernel(swe_mesh_t m, swe_state_t s, swe_sources_t src, Phys p, float cfl, int all_active,
+                            uint32_t n_steps) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ TiledShared sh;
+    __shared__ int flag[2];
+    GridSync g{s.sync, s.sync + 32, 0u};
+    if (threadIdx.x == 0) {
+        mbar_init(reinterpret_cast<uint64_t *>(smem), 1u);
+        mbar_init(reinterpret_cast<uint64_t *>(smem) + 1, 1u);
+        fence_barrier_init();
+        g.epoch = ld_acquire_u32(g.gen);
+    }
+    __syncthreads();
+    const uint32_t first = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    auto nothing = [] {};
+    auto control = [&] {
+        // every instance's step control, then the new lists become current
+        for (uint32_t i = threadIdx.x; i < m.n_inst; i += blockDim.x)
+            step_control(s.ctrl + i, s.dt_buf + kDtWords * i, 1);
+        if (threadIdx.x == 0) {
+            volatile uint32_t *sched = s.sched;
+            sched[kSchedActive] = sched[kSchedNext];
+            sched[kSchedItems] = sched[kSchedNextItems];
+            sched[kSchedNext] = 0u;
+            sched[kSchedNextItems] = 0u;
+        }
+    };
+    uint32_t k = 0;
+    uint64_t computed = 0;
+    bool ok = true;
+    for (uint32_t step = 0; step < n_steps; ++step) {
+        if (!(ok = tiled_pass<0, COMP, CLAMP>(m, s, p, cfl, smem, sh, k, computed))) break;
+        if (!(ok = grid_sync(g, flag, nothing))) break;
+        if (!(ok = tiled_pass<1, COMP, CLAMP>(m, s, p, cfl, smem, sh, k, computed))) break;
+        if (!(ok = grid_sync(g, flag, nothing))) break;
+        if (src.count) {
+            source_apply(m, s, src, p.dry_tol, COMP ? 1 : 0, first, stride);
+            if (!(ok = grid_sync(g, flag, nothing))) break;
+            source_bound(m, s, src, p, cfl, first, stride);
+            if (!(ok = grid_sync(g, flag, nothing))) break;
+        }
+        dilate_pass(m, s, all_active);
+        if (!(ok = grid_sync(g, flag, control))) break;
+    }
+    if (threadIdx.x == 0) {
+        if (!ok) atomicOr(&s.ctrl->error, 2u);
+        if (computed) atomicAdd(reinterpret_cast<unsigned long long *>(s.sched + kSchedComputed), computed);
+    }
+}
+
+template <bool COMP, bool CLAMP>
+int launch_persistent(const swe_mesh_t *m, const swe_state_t *s, const swe_params_t *p, const swe_sources_t *src,
+                      uint32_t n_steps, cudaStream_t st) {
+    auto kern = persistent_steps_kernel<COMP, CLAMP>;
+    const size_t bytes = tile_plan(m->max_sub_edges, m->max_sub_slots, 10u).total;
+    int rc = set_smem(kern, bytes);
+    if (rc) return rc;
+    int per_sm = 0, dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTileThreads, bytes) != cudaSuccess)
+        return SWE_ERR_CUDA;
+    if (per_sm < 1) return SWE_ERR_TOO_LARGE;
+    const uint32_t fit = static_cast<uint32_t>(per_sm) * static_cast<uint32_t>(sms);
+    const uint32_t grid = (p->grid == 0u || p->grid > fit) ? fit : p->grid;
+    Phys ph{p->g, p->dry_tol};
+    float cfl = p->cfl;
+    int all_active = p->active_set ? 0 : 1;
+    swe_mesh_t mm = *m;
+    swe_state_t ss = *s;
+    swe_sources_t sc = *src;
+    void *args[] = {&mm, &ss, &sc, &ph, &cfl, &all_active, &n_steps};
+    if (cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(kern), dim3(grid), dim3(kTileThreads), args, bytes,
+                                    st) != cudaSuccess)
+        return SWE_ERR_CUDA;
+    return SWE_OK;
+}
+
+int configure_persistent(const swe_mesh_t *mesh, int *blocks_per_sm) {
+    const size_t bytes = tile_plan(mesh->max_sub_edges, mesh->max_sub_slots, 10u).total;
+    int rc = set_smem(persistent_steps_kernel<true, false>, bytes);
+    if (!rc) rc = set_smem(persistent_steps_kernel<true, true>, bytes);
+    if (!rc) rc = set_smem(persistent_steps_kernel<false, false>, bytes);
+    if (!rc) rc = set_smem(persistent_steps_kernel<false, true>, bytes);
+    if (rc) return rc;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, persistent_steps_kernel<true, false>,
+                                                         kTileThreads, bytes) == cudaSuccess
+               ? SWE_OK
+               : SWE_ERR_CUDA;
+}
+
+}  // namespace swe
+
+using namespace swe;
+
+extern "C" int swe_steps(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params_t *params,
+                         const swe_sources_t *sources, uint32_t n_steps, swe_stream_t stream) {
+    if (!mesh_ok(mesh) || !state_ok(state) || !params || !sources || params->kernel > 2u) return SWE_ERR_ARGUMENT;
+    if (n_steps == 0u) return SWE_OK;
+    if (params->kernel < 2u) {
+        for (uint32_t k = 0; k < n_steps; ++k) {
+            const int rc = swe_step(mesh, state, params, sources, stream);
+            if (rc) return rc;
+        }
+        return SWE_OK;
+    }
+    if (!state->sync) return SWE_ERR_ARGUMENT;
+    if (mesh->max_sub_edges > 2047u || mesh->max_sub_slots > 2047u || mesh->n_inst > 1023u) return SWE_ERR_TOO_LARGE;
+    if (sources->count && (!sources->cells || !sources->rate)) return SWE_ERR_ARGUMENT;
+    if (params->compensated)
+        return params->track_clamp ? launch_persistent<true, true>(mesh, state, params, sources, n_steps, stream)
+                                   : launch_persistent<true, false>(mesh, state, params, sources, n_steps, stream);
+    return params->track_clamp ? launch_persistent<false, true>(mesh, state, params, sources, n_steps, stream)
+                               : launch_persistent<false, false>(mesh, state, params, sources, n_steps, stream);
+}

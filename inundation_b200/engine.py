@@ -44,7 +44,7 @@ RESIDENT_CTRL_DTYPE = np.dtype(
 
 START, STEP, RETARGET = 0, 1, 2
 STATE_ARRAYS = ("h", "hu", "hv", "h_lo", "h1", "hu1", "hv1", "h1_lo", "clamp_mass")
-KERNELS = {"tiled": 0, "plain": 1}
+KERNELS = {"tiled": 0, "plain": 1, "persistent": 2}
 
 
 def _i32(a: NDArray) -> NDArray[np.int32]:
@@ -60,8 +60,9 @@ class ResidentEngine:
     compensated: bool = True
     track_clamp: bool = False
     cfl_safety: float = 1.0
-    # Stage kernel: "tiled" (64-cell tiles from the dilation's work items, staged by bulk copies)
-    # or "plain" (256-cell blocks, direct loads).
+    # Stage kernel: "tiled" (64-cell tiles from the dilation's work items, staged by bulk copies),
+    # "plain" (256-cell blocks, direct loads) or "persistent" (the tiled stages and the rest of the
+    # step in one cooperative launch per submit, phases separated by grid barriers).
     stage_kernel: str = "tiled"
 
     def _init_engine(
@@ -137,7 +138,7 @@ class ResidentEngine:
         """Persistent CTAs of a stage kernel: CTAs per SM x SMs, at most one per work unit."""
         kernel = self._kernel if kernel is None else kernel
         per_sm = self._per_sm[kernel] if self.ctas_per_sm is None else min(self.ctas_per_sm, self._per_sm[kernel])
-        units = 4 * self.n_blocks if kernel == 0 else self.n_blocks  # the tiled kernel works on 64-cell tiles
+        units = self.n_blocks if kernel == 1 else 4 * self.n_blocks  # 64-cell tiles, or 256-cell blocks
         grid = min(units, per_sm * self._sms)
         if self.max_grid is not None:
             grid = min(grid, self.max_grid)
@@ -160,6 +161,7 @@ class ResidentEngine:
         dt[1::4] = np.float32(1e30).view(np.uint32)
         self._dt_buf = self._dev(dt.view(np.int32))
         self._ctrl_dev = torch.zeros(6 * ni, dtype=torch.int64, device=dev)
+        self._sync = torch.zeros(64, dtype=torch.int32, device=dev)  # grid barrier words of the persistent kernel
         self._ctrl_pinned = torch.zeros(6 * ni, dtype=torch.int64).pin_memory()
         self._ctrl = self._ctrl_pinned.numpy().view(RESIDENT_CTRL_DTYPE)
         self._partials = torch.zeros(int(self._lib.swe_volume_partials(n)), dtype=torch.float64, device=dev)
@@ -173,6 +175,7 @@ class ResidentEngine:
         s.sched = self._sched.data_ptr()
         s.dt_buf = self._dt_buf.data_ptr()
         s.ctrl = self._ctrl_dev.data_ptr()
+        s.sync = self._sync.data_ptr()
         self._state = s
 
     def _params(self) -> native.SweParams:
@@ -373,11 +376,13 @@ class ResidentEngine:
         mesh, state = ctypes.byref(self._mesh), ctypes.byref(self._state)
         pp, sp = ctypes.byref(params), ctypes.byref(sources)
         stream = ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
-        for _ in range(n_steps):
-            native.check(self._lib.swe_step(mesh, state, pp, sp, stream), "swe_step")
+        native.check(self._lib.swe_steps(mesh, state, pp, sp, n_steps, stream), "swe_steps")
 
-    def _graph(self, steps: int | None = None) -> torch.cuda.CUDAGraph:
+    def _graph(self, steps: int | None = None):
+        """A replayable submit of ``steps`` steps: a CUDA graph, or for the persistent kernel its one launch."""
         steps = self.steps_per_graph if steps is None else steps
+        if self._kernel == KERNELS["persistent"]:
+            return _PersistentSubmit(self, steps)
         key = (
             steps,
             bool(self.compensated),
@@ -404,6 +409,22 @@ class ResidentEngine:
         graph = self._graph()
         with torch.cuda.stream(self._stream):
             graph.replay()
+
+
+class _PersistentSubmit:
+    """One cooperative launch of the persistent kernel per replay (its own grid barriers replace the graph)."""
+
+    def __init__(self, engine: ResidentEngine, steps: int) -> None:
+        self.engine, self.steps = engine, steps
+        self.params, self.sources = engine._params(), engine._sources()
+
+    def replay(self) -> None:
+        e = self.engine
+        native.check(
+            e._lib.swe_steps(ctypes.byref(e._mesh), ctypes.byref(e._state), ctypes.byref(self.params),
+                             ctypes.byref(self.sources), self.steps, e._cuda_stream),
+            "swe_steps",
+        )
 
 
 __all__ = ["KERNELS", "NO_HYDROGRAPH", "RESIDENT_CTRL_DTYPE", "Hydrograph", "ResidentEngine", "START", "STEP", "RETARGET"]

@@ -34,6 +34,7 @@ _SIGNATURES: dict[str, tuple[list, object]] = {
     "swe_step_control": ([_P, _P, _U32, ctypes.c_int, _P], ctypes.c_int),
     "swe_prologue": ([_P, _P, _P, _P], ctypes.c_int),
     "swe_step": ([_P, _P, _P, _P, _P], ctypes.c_int),
+    "swe_steps": ([_P, _P, _P, _P, _U32, _P], ctypes.c_int),
     "swe_volume_partials": ([_U32], _U32),
     "swe_volume_fp64": ([_P, _P, _P, _U32, _P, _P, _P], ctypes.c_int),
     "swe_volume_fp64_noalloc": ([_P, _P, _P, _U32, _P, _P], ctypes.c_int),
@@ -72,7 +73,7 @@ class SweState(ctypes.Structure):
         (name, _P)
         for name in (
             "h", "hu", "hv", "h_lo", "h1", "hu1", "hv1", "h1_lo", "clamp_mass", "blk", "active_list", "items",
-            "sched", "dt_buf", "ctrl",
+            "sched", "dt_buf", "ctrl", "sync",
         )
     ]
 

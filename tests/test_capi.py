@@ -68,7 +68,7 @@ def test_status_strings_and_argument_checks(lib: ctypes.CDLL) -> None:
 
 def test_ctypes_structs_match_the_header_layout() -> None:
     assert ctypes.sizeof(native.SweMesh) == 16 + 17 * 8 + 8 + 11 * 8
-    assert ctypes.sizeof(native.SweState) == 15 * 8
+    assert ctypes.sizeof(native.SweState) == 16 * 8
     assert ctypes.sizeof(native.SweParams) == 32
     assert ctypes.sizeof(native.SweSources) == 7 * 8 + 8
 

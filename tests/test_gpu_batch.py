@@ -71,7 +71,7 @@ def batch_case():
     return solver, ms
 
 
-@pytest.mark.parametrize("kernel", ["tiled", "plain"])
+@pytest.mark.parametrize("kernel", ["tiled", "plain", "persistent"])
 def test_every_instance_matches_its_own_oracle_run(kernel: str, batch_case) -> None:
     solver, ms = batch_case
     solver.stage_kernel = kernel
@@ -142,10 +142,10 @@ def test_fixed_step_runs_and_autotuner_keep_results() -> None:
         m.h0 = np.where(np.arange(m.geom.N) < m.geom.N // 5, 0.3, 0.0).astype(np.float32)
     solver = BatchedSolver(ms)
     choice = autotune(solver, dt_max=1.0, dt_init=0.01, steps=20)
-    assert {r["stage_kernel"] for r in choice["results"]} == {"tiled", "plain"}
+    assert {r["stage_kernel"] for r in choice["results"]} == {"tiled", "plain", "persistent"}
     assert solver.stage_kernel == choice["stage_kernel"]
     outs = []
-    for kernel in ("tiled", "plain"):
+    for kernel in ("tiled", "plain", "persistent"):
         solver.stage_kernel = kernel
         solver.reset()
         solver.start(dt_max=1.0, dt_init=0.01)
@@ -153,8 +153,9 @@ def test_fixed_step_runs_and_autotuner_keep_results() -> None:
         solver.run_steps(100)
         assert (solver.steps == 100).all()
         outs.append([solver.download_h(i) for i in range(3)])
-    for a, b in zip(*outs, strict=True):
-        np.testing.assert_array_equal(bits(a), bits(b))
+    for other in outs[1:]:
+        for a, b in zip(outs[0], other, strict=True):
+            np.testing.assert_array_equal(bits(a), bits(b))
     for i, s in enumerate(scs):
         o = ResidentOracle(s.geom, ms[i].h0, s.hu0, s.hv0, s.manning, steps_per_graph=100)
         o.set_sources(None, s.hydrographs)
