@@ -21,7 +21,8 @@ namespace swe {
 constexpr int kBlockCells = 256;
 constexpr int kThreads = 256;
 constexpr int kTileCells = 64;
-constexpr int kTileThreads = 128;
+constexpr int kTileThreads = 128;     // threads of a tile CTA of the tiled stage kernel
+constexpr int kPersistThreads = 256;  // threads of a tile CTA of the persistent kernel: one edge record each
 constexpr uint32_t kBlkWords = 3, kBlkWet = 0, kBlkActive = 1, kBlkForced = 2;
 constexpr uint32_t kNoBound = 0xFFFFFFFFu;
 constexpr uint32_t kDtWords = 4;

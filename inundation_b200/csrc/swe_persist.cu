@@ -75,66 +75,53 @@ __device__ __forceinline__ bool grid_sync(GridSync &g, int *flag, F last) {
 
 // Dilation of the wet marks over each block's two-ring and compaction into the
 // next step's block list and tile work items (the dilate_compact kernel's work):
-// one lane per block, 32 blocks per warp, one pair of atomics per warp.
+// one warp per block, its lanes reading the two-ring in parallel, one pair of
+// atomics per active block.
 __device__ __forceinline__ void dilate_pass(const swe_mesh_t &m, const swe_state_t &s, int all_active) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-    for (uint32_t chunk = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); chunk * 32u < m.n_blocks;
-         chunk += warps) {
-        const uint32_t b = chunk * 32u + lane;
-        uint32_t v = 0u;
-        if (b < m.n_blocks && s.dt_buf[kDtWords * m.block_inst[b]] != 0u) {
-            if (all_active) {
-                v = 1u;
-            } else {
-                v = s.blk[kBlkWords * b + kBlkWet] | s.blk[kBlkWords * b + kBlkForced];
-                for (uint32_t k = m.ring_ptr[b], k1 = m.ring_ptr[b + 1]; k < k1 && v == 0u; ++k) {
-                    const uint32_t nb = m.ring_idx[k];
-                    v = s.blk[kBlkWords * nb + kBlkWet] | s.blk[kBlkWords * nb + kBlkForced];
-                }
-                v = v ? 1u : 0u;
+    for (uint32_t b = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); b < m.n_blocks; b += warps) {
+        if (s.dt_buf[kDtWords * m.block_inst[b]] == 0u) continue;  // a no-op step keeps its flags
+        uint32_t v;
+        if (all_active) {
+            v = 1u;
+        } else {
+            const uint32_t k0 = m.ring_ptr[b], k1 = m.ring_ptr[b + 1];
+            v = (lane == 0) ? (s.blk[kBlkWords * b + kBlkWet] | s.blk[kBlkWords * b + kBlkForced]) : 0u;
+            for (uint32_t k = k0 + lane; k < k1; k += 32) {
+                const uint32_t nb = m.ring_idx[k];
+                v |= s.blk[kBlkWords * nb + kBlkWet] | s.blk[kBlkWords * nb + kBlkForced];
             }
-            s.blk[kBlkWords * b + kBlkActive] = v;
+            v = __any_sync(0xFFFFFFFFu, v != 0u) ? 1u : 0u;
         }
-        const bool on = v != 0u;
-        const uint32_t cells = on ? m.block_cells[b] : 0u;
+        if (lane == 0) s.blk[kBlkWords * b + kBlkActive] = v;
+        if (!v) continue;
+        const uint32_t cells = m.block_cells[b];
         const uint32_t n_items = (cells + kTileCells - 1) / kTileCells;
-        const unsigned ballot = __ballot_sync(0xFFFFFFFFu, on);
-        uint32_t before = n_items;
-        for (int d = 1; d < 32; d <<= 1) {
-            const uint32_t up = __shfl_up_sync(0xFFFFFFFFu, before, d);
-            if (static_cast<int>(lane) >= d) before += up;
-        }
-        const uint32_t total = __shfl_sync(0xFFFFFFFFu, before, 31);
-        before -= n_items;
         uint32_t pos = 0, ipos = 0;
-        if (lane == 0 && ballot) {
-            pos = atomicAdd(&s.sched[kSchedNext], static_cast<uint32_t>(__popc(ballot)));
-            ipos = atomicAdd(&s.sched[kSchedNextItems], total);
+        if (lane == 0) {
+            pos = atomicAdd(&s.sched[kSchedNext], 1u);
+            ipos = atomicAdd(&s.sched[kSchedNextItems], n_items);
         }
         pos = __shfl_sync(0xFFFFFFFFu, pos, 0);
-        ipos = __shfl_sync(0xFFFFFFFFu, ipos, 0) + before;
-        if (on) {
-            const uint32_t slot = pos + __popc(ballot & ((1u << lane) - 1u));
-            if (slot < m.n_blocks) s.active_list[slot] = b;
-            const uint32_t inst = m.block_inst[b];
-            uint4 *out = reinterpret_cast<uint4 *>(s.items);
-            for (uint32_t q = 0; q < n_items && ipos + q < 4u * m.n_blocks; ++q) {
-                const uint32_t t = 4u * b + q;
-                const uint32_t l0 = m.sub_lcsr_ptr[t];
-                out[ipos + q] = make_item(t, min(static_cast<uint32_t>(kTileCells), cells - q * kTileCells),
-                                          m.sub_ptr[t], l0, m.sub_count[t], m.sub_lcsr_ptr[t + 1] - l0, inst);
-            }
+        ipos = __shfl_sync(0xFFFFFFFFu, ipos, 0);
+        if (lane == 0 && pos < m.n_blocks) s.active_list[pos] = b;
+        if (lane < n_items && ipos + lane < 4u * m.n_blocks) {
+            const uint32_t t = 4u * b + lane;
+            const uint32_t l0 = m.sub_lcsr_ptr[t];
+            reinterpret_cast<uint4 *>(s.items)[ipos + lane] =
+                make_item(t, min(static_cast<uint32_t>(kTileCells), cells - lane * kTileCells), m.sub_ptr[t], l0,
+                          m.sub_count[t], m.sub_lcsr_ptr[t + 1] - l0, m.block_inst[b]);
         }
     }
 }
 
 template <bool COMP, bool CLAMP>
-__global__ void __launch_bounds__(kTileThreads)
+__global__ void __launch_bounds__(kPersistThreads, 1024 / kPersistThreads)
     persistent_steps_kernel(swe_mesh_t m, swe_state_t s, swe_sources_t src, Phys p, float cfl, int all_active,
                             uint32_t n_steps) {
     extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ TiledShared sh;
+    __shared__ TiledShared<kPersistThreads> sh;
     __shared__ int flag[2];
     GridSync g{s.sync, s.sync + 32, 0u};
     if (threadIdx.x == 0) {
@@ -162,9 +149,9 @@ __global__ void __launch_bounds__(kTileThreads)
     uint64_t computed = 0;
     bool ok = true;
     for (uint32_t step = 0; step < n_steps; ++step) {
-        if (!(ok = tiled_pass<0, COMP, CLAMP>(m, s, p, cfl, smem, sh, k, computed))) break;
+        if (!(ok = tiled_pass<0, COMP, CLAMP, kPersistThreads>(m, s, p, cfl, smem, sh, k, computed))) break;
         if (!(ok = grid_sync(g, flag, nothing))) break;
-        if (!(ok = tiled_pass<1, COMP, CLAMP>(m, s, p, cfl, smem, sh, k, computed))) break;
+        if (!(ok = tiled_pass<1, COMP, CLAMP, kPersistThreads>(m, s, p, cfl, smem, sh, k, computed))) break;
         if (!(ok = grid_sync(g, flag, nothing))) break;
         if (src.count) {
             source_apply(m, s, src, p.dry_tol, COMP ? 1 : 0, first, stride);
@@ -191,7 +178,7 @@ int launch_persistent(const swe_mesh_t *m, const swe_state_t *s, const swe_param
     int per_sm = 0, dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTileThreads, bytes) != cudaSuccess)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPersistThreads, bytes) != cudaSuccess)
         return SWE_ERR_CUDA;
     if (per_sm < 1) return SWE_ERR_TOO_LARGE;
     const uint32_t fit = static_cast<uint32_t>(per_sm) * static_cast<uint32_t>(sms);
@@ -203,7 +190,7 @@ int launch_persistent(const swe_mesh_t *m, const swe_state_t *s, const swe_param
     swe_state_t ss = *s;
     swe_sources_t sc = *src;
     void *args[] = {&mm, &ss, &sc, &ph, &cfl, &all_active, &n_steps};
-    if (cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(kern), dim3(grid), dim3(kTileThreads), args, bytes,
+    if (cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(kern), dim3(grid), dim3(kPersistThreads), args, bytes,
                                     st) != cudaSuccess)
         return SWE_ERR_CUDA;
     return SWE_OK;
@@ -217,7 +204,7 @@ int configure_persistent(const swe_mesh_t *mesh, int *blocks_per_sm) {
     if (!rc) rc = set_smem(persistent_steps_kernel<false, true>, bytes);
     if (rc) return rc;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, persistent_steps_kernel<true, false>,
-                                                         kTileThreads, bytes) == cudaSuccess
+                                                         kPersistThreads, bytes) == cudaSuccess
                ? SWE_OK
                : SWE_ERR_CUDA;
 }

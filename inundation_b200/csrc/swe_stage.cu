@@ -143,7 +143,7 @@ template <int STAGE, bool COMP, bool CLAMP>
 __global__ void __launch_bounds__(kTileThreads, 8) stage_tiled_kernel(swe_mesh_t m, swe_state_t s, Phys p, float cfl) {
     if (blockIdx.x >= s.sched[kSchedItems]) return;
     extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ TiledShared sh;
+    __shared__ TiledShared<kTileThreads> sh;
     if (threadIdx.x == 0) {
         mbar_init(reinterpret_cast<uint64_t *>(smem), 1u);
         mbar_init(reinterpret_cast<uint64_t *>(smem) + 1, 1u);
@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(kTileThreads, 8) stage_tiled_kernel(swe_mesh_t
     __syncthreads();
     uint32_t k = 0;
     uint64_t computed = 0;
-    if (!tiled_pass<STAGE, COMP, CLAMP>(m, s, p, cfl, smem, sh, k, computed)) return;
+    if (!tiled_pass<STAGE, COMP, CLAMP, kTileThreads>(m, s, p, cfl, smem, sh, k, computed)) return;
     if (STAGE == 1 && threadIdx.x == 0 && computed)
         atomicAdd(reinterpret_cast<unsigned long long *>(s.sched + kSchedComputed), computed);
 }

@@ -199,8 +199,9 @@ __device__ __forceinline__ void tile_issue(const swe_mesh_t &m, const swe_state_
 }
 
 // Shared words of a tile pass besides the staged buffers.
+template <int TPB>
 struct TiledShared {
-    uint32_t red[kTileThreads / 32];
+    uint32_t red[TPB / 32];
     uint4 items[2];
     uint32_t dts[2];
 };
@@ -211,9 +212,9 @@ struct TiledShared {
 // phases); computed cells of the corrector accumulate in `computed`.
 // Returns false when staged data did not arrive within the wait bound (the
 // copies in flight have had one more bounded wait; the caller must stop).
-template <int STAGE, bool COMP, bool CLAMP>
+template <int STAGE, bool COMP, bool CLAMP, int TPB>
 __device__ bool tiled_pass(const swe_mesh_t &m, const swe_state_t &s, const Phys &p, float cfl, unsigned char *smem,
-                           TiledShared &sh, uint32_t &k, uint64_t &computed) {
+                           TiledShared<TPB> &sh, uint32_t &k, uint64_t &computed) {
     const uint32_t count = *reinterpret_cast<volatile const uint32_t *>(s.sched + kSchedItems);
     if (blockIdx.x >= count) return true;
     constexpr uint32_t nc = STAGE ? 10u : 6u;
@@ -264,7 +265,7 @@ __device__ bool tiled_pass(const swe_mesh_t &m, const swe_state_t &s, const Phys
             const int base = static_cast<int>(it.tile * kTileCells);
 
             // Edge fluxes, written in place over the consumed records.
-            for (uint32_t j = tid; j < it.ne; j += kTileThreads) {
+            for (uint32_t j = tid; j < it.ne; j += TPB) {
                 const int cL = B.cl[j], cR = B.cr[j];
                 const float nx = B.nx[j], ny = B.ny[j];
                 float hL, huL, hvL, hR, huR, hvR;
