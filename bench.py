@@ -60,7 +60,8 @@ def parse_args() -> argparse.Namespace:
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--chunk", type=int, default=500, help="steps per captured graph in the timed region")
-    ap.add_argument("--kernel", choices=["tiled", "plain", "persistent"], default="tiled", help="stage kernel variant")
+    ap.add_argument("--kernel", choices=["auto", "tiled", "plain", "persistent"], default="auto",
+                    help="stage kernel variant (auto: by the active fraction after the prologue)")
     ap.add_argument("--ctas-per-sm", type=int, default=None, help="persistent CTAs per SM of the stage kernel")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-scenarios measurement")
     ap.add_argument("--batch-count", type=int, default=64, help="scenarios in the batched measurement")
@@ -323,6 +324,11 @@ def run_b200(args, world: int, rank: int, local: int) -> None:
     solver.stage_kernel = args.kernel
     solver.ctas_per_sm = args.ctas_per_sm
     plan(solver, sc)
+    if args.kernel == "auto":  # the choice "auto" makes for this state, fixed for the timed region
+        from inundation_b200.engine import KERNELS
+
+        args.kernel = {v: k for k, v in KERNELS.items()}[solver._kernel]
+        solver.stage_kernel = args.kernel
     warm, _ = capture_chunks(solver, args.warmup, args.chunk, timed=False)
     graphs, events = capture_chunks(solver, args.steps, args.chunk, timed=True)
     for gr in warm:

@@ -60,6 +60,8 @@ class GaugeCalibration(ResidentEngine):
     """
 
     cut_depth: float = 0.0
+    # the segment graphs capture one swe_step per step: a per-step stage kernel
+    stage_kernel: str = "tiled"
 
     def __init__(
         self,

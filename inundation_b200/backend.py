@@ -211,7 +211,7 @@ class SWESolverB200Resident(ResidentEngine):
         ctrl["dt_max_ticks"] = dt_max_ticks
         ctrl["dry_dt_ticks"] = dry_dt_ticks
         ctrl["cfl_safety"] = self.cfl_safety
-        graph = self._graph()
+        self._graph()  # capture before the first window
         planned = False
         wall0 = _time.monotonic()
         last_log = wall0
@@ -227,6 +227,7 @@ class SWESolverB200Resident(ResidentEngine):
             self._read_ctrl()
             while int(ctrl["now_ticks"][0]) < stop:
                 before = int(ctrl["now_ticks"][0])
+                graph = self._graph()  # per submit: "auto" may change kernel with the active fraction
                 with torch.cuda.stream(self._stream):
                     graph.replay()
                 self._read_ctrl()

@@ -45,6 +45,9 @@ RESIDENT_CTRL_DTYPE = np.dtype(
 START, STEP, RETARGET = 0, 1, 2
 STATE_ARRAYS = ("h", "hu", "hv", "h_lo", "h1", "hu1", "hv1", "h1_lo", "clamp_mass")
 KERNELS = {"tiled": 0, "plain": 1, "persistent": 2}
+# "auto": the persistent kernel while few blocks are active (its phases are latency-bound), the
+# 256-cell block kernel once more than this fraction of blocks is active (issue-bound work).
+AUTO_DENSE_FRACTION = 0.25
 
 
 def _i32(a: NDArray) -> NDArray[np.int32]:
@@ -61,9 +64,10 @@ class ResidentEngine:
     track_clamp: bool = False
     cfl_safety: float = 1.0
     # Stage kernel: "tiled" (64-cell tiles from the dilation's work items, staged by bulk copies),
-    # "plain" (256-cell blocks, direct loads) or "persistent" (the tiled stages and the rest of the
-    # step in one cooperative launch per submit, phases separated by grid barriers).
-    stage_kernel: str = "tiled"
+    # "plain" (256-cell blocks, direct loads), "persistent" (the tiled stages and the rest of the
+    # step in one cooperative launch per submit, phases separated by grid barriers) or "auto"
+    # (persistent or plain by the active fraction read after every submit). All give the same bits.
+    stage_kernel: str = "auto"
 
     def _init_engine(
         self,
@@ -146,8 +150,11 @@ class ResidentEngine:
 
     @property
     def _kernel(self) -> int:
+        if self.stage_kernel == "auto":
+            dense = self._active_blocks > AUTO_DENSE_FRACTION * self.n_blocks
+            return KERNELS["plain"] if dense else KERNELS["persistent"]
         if self.stage_kernel not in KERNELS:
-            raise ValueError(f"stage_kernel must be one of {sorted(KERNELS)}, got {self.stage_kernel!r}")
+            raise ValueError(f"stage_kernel must be one of {sorted(KERNELS)} or 'auto', got {self.stage_kernel!r}")
         return KERNELS[self.stage_kernel]
 
     def _alloc_state(self) -> None:
@@ -164,6 +171,8 @@ class ResidentEngine:
         self._sync = torch.zeros(64, dtype=torch.int32, device=dev)  # grid barrier words of the persistent kernel
         self._ctrl_pinned = torch.zeros(6 * ni, dtype=torch.int64).pin_memory()
         self._ctrl = self._ctrl_pinned.numpy().view(RESIDENT_CTRL_DTYPE)
+        self._sched_pinned = torch.zeros(8, dtype=torch.int64).pin_memory()
+        self._active_blocks = 0  # blocks in the current active list, as of the last control-block read
         self._partials = torch.zeros(int(self._lib.swe_volume_partials(n)), dtype=torch.float64, device=dev)
         self._volume = torch.zeros(1, dtype=torch.float64, device=dev)
         s = native.SweState()
@@ -338,10 +347,13 @@ class ResidentEngine:
     def _read_ctrl(self) -> None:
         with torch.cuda.stream(self._stream):
             self._ctrl_pinned.copy_(self._ctrl_dev, non_blocking=True)
+            self._sched_pinned.copy_(self._sched, non_blocking=True)
         self._stream.synchronize()
+        self._active_blocks = int(self._sched_pinned.numpy().view(np.uint32)[0])
         err = int(self._ctrl["error"].max())
         if err:
-            raise RuntimeError(f"{B200_BACKEND}: a bounded device wait for staged data timed out (error {err})")
+            what = {1: "for staged data", 2: "at a grid barrier"}.get(err & 3, "")
+            raise RuntimeError(f"{B200_BACKEND}: a bounded device wait {what} timed out (error {err})")
 
     def _enqueue_prologue(self) -> None:
         p = self._params()
