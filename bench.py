@@ -377,8 +377,8 @@ def run_b200(args, world: int, rank: int, local: int) -> None:
     peak, peak_kind = peaks()
     traffic = None
     tfile = ROOT / "profiles" / "stage_kernel_traffic.json"
-    if tfile.exists():
-        per_cell = json.loads(tfile.read_text()).get("dram_bytes_per_computed_cell_step")
+    if tfile.exists():  # ncu DRAM bytes per computed cell-step of this kernel, scaled to a launch
+        per_cell = json.loads(tfile.read_text()).get(args.kernel, {}).get("dram_bytes_per_computed_cell_step")
         if per_cell:
             traffic = per_cell * computed / launches
     value = world * g.N * args.steps / (ms_max * 1e-3)
