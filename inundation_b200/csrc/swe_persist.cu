@@ -149,9 +149,9 @@ __global__ void __launch_bounds__(kPersistThreads, 1024 / kPersistThreads)
     uint64_t computed = 0;
     bool ok = true;
     for (uint32_t step = 0; step < n_steps; ++step) {
-        if (!(ok = tiled_pass<0, COMP, CLAMP, kPersistThreads>(m, s, p, cfl, smem, sh, k, computed))) break;
+        if (!(ok = tiled_pass<0, COMP, CLAMP, kPersistThreads, true>(m, s, p, cfl, smem, sh, k, computed))) break;
         if (!(ok = grid_sync(g, flag, nothing))) break;
-        if (!(ok = tiled_pass<1, COMP, CLAMP, kPersistThreads>(m, s, p, cfl, smem, sh, k, computed))) break;
+        if (!(ok = tiled_pass<1, COMP, CLAMP, kPersistThreads, true>(m, s, p, cfl, smem, sh, k, computed))) break;
         if (!(ok = grid_sync(g, flag, nothing))) break;
         if (src.count) {
             source_apply(m, s, src, p.dry_tol, COMP ? 1 : 0, first, stride);
@@ -172,7 +172,7 @@ template <bool COMP, bool CLAMP>
 int launch_persistent(const swe_mesh_t *m, const swe_state_t *s, const swe_params_t *p, const swe_sources_t *src,
                       uint32_t n_steps, cudaStream_t st) {
     auto kern = persistent_steps_kernel<COMP, CLAMP>;
-    const size_t bytes = tile_plan(m->max_sub_edges, m->max_sub_slots, 10u).total;
+    const size_t bytes = tiled_smem_bytes(m->max_sub_edges, m->max_sub_slots, true);
     int rc = set_smem(kern, bytes);
     if (rc) return rc;
     int per_sm = 0, dev = 0, sms = 0;
@@ -197,7 +197,7 @@ int launch_persistent(const swe_mesh_t *m, const swe_state_t *s, const swe_param
 }
 
 int configure_persistent(const swe_mesh_t *mesh, int *blocks_per_sm) {
-    const size_t bytes = tile_plan(mesh->max_sub_edges, mesh->max_sub_slots, 10u).total;
+    const size_t bytes = tiled_smem_bytes(mesh->max_sub_edges, mesh->max_sub_slots, true);
     int rc = set_smem(persistent_steps_kernel<true, false>, bytes);
     if (!rc) rc = set_smem(persistent_steps_kernel<true, true>, bytes);
     if (!rc) rc = set_smem(persistent_steps_kernel<false, false>, bytes);

@@ -17,7 +17,7 @@ template <int STAGE, bool COMP, bool CLAMP>
 __device__ __forceinline__ void update_cell(const swe_state_t &s, const Phys &p, float cfl, float dt, uint32_t i,
                                             float A, float n, float hi, float hui, float hvi, float loi, float h0,
                                             float hu0, float hv0, float lo0, float sdh, float sdhu, float sdhv,
-                                            float lam, bool &wet, uint32_t &bound) {
+                                            float lam, bool &wet, uint32_t &bound, float *keep = nullptr) {
     const float dti = dt / A;
     float h_new, lo_new, h_raw;
     if (COMP) {
@@ -53,6 +53,12 @@ __device__ __forceinline__ void update_cell(const swe_state_t &s, const Phys &p,
         if (COMP) s.h1_lo[i] = lo_new;
         s.hu1[i] = hu_new;
         s.hv1[i] = hv_new;
+        if (keep) {  // the predictor's state kept in shared memory, columns h, hu, hv, h_lo
+            keep[0] = h_new;
+            keep[kTileCells] = hu_new;
+            keep[2 * kTileCells] = hv_new;
+            keep[3 * kTileCells] = lo_new;
+        }
         return;
     }
     float hf;
@@ -204,35 +210,179 @@ struct TiledShared {
     uint32_t red[TPB / 32];
     uint4 items[2];
     uint32_t dts[2];
+    uint32_t count;
 };
+
+// Shared-memory bytes of a tile pass: two staged buffers, and with KEEP the
+// flux words in arrays of their own (7 per record).
+__host__ __device__ inline size_t tiled_smem_bytes(uint32_t max_edges, uint32_t max_slots, bool keep) {
+    const TilePlan L = tile_plan(max_edges, max_slots, 10u);
+    return keep ? L.total + 7u * L.capE * 4u : L.total;
+}
+
+// Fluxes, gather and update of one staged tile. The stage's input state is in
+// columns in_col..in_col+3 of B.c (h, hu, hv, h_lo), the committed state of the
+// corrector in com_col..com_col+3. F == nullptr: the flux words overwrite the
+// consumed records; otherwise they go to F (7 x capE words) and the records stay.
+template <int STAGE, bool COMP, bool CLAMP, int TPB>
+__device__ __forceinline__ void tile_compute(const swe_mesh_t &m, const swe_state_t &s, const Phys &p, float cfl,
+                                             const TileBuf &B, const Item &it, float dt, uint32_t in_col,
+                                             uint32_t com_col, float *F, uint32_t capE, uint32_t *red,
+                                             uint64_t &computed, bool keep_pred) {
+    const uint32_t tid = threadIdx.x;
+    const uint32_t b = it.tile >> 2;
+    if (STAGE == 0 && (it.tile & 3u) == 0u && tid == 0) s.blk[kBlkWords * b + kBlkWet] = 0u;
+    const float *C0 = B.c + in_col * kTileCells, *C1 = C0 + kTileCells, *C2 = C0 + 2 * kTileCells;
+    const int base = static_cast<int>(it.tile * kTileCells);
+    int32_t *live_w = F ? reinterpret_cast<int32_t *>(F) : B.cr;
+    float *W0 = F ? F + capE : B.nx, *W1 = F ? F + 2 * capE : B.ny, *W2 = F ? F + 3 * capE : B.len;
+    float *W3 = F ? F + 4 * capE : B.dzl, *W4 = F ? F + 5 * capE : B.dzr;
+    int32_t *W5 = F ? reinterpret_cast<int32_t *>(F + 6 * capE) : B.cl;
+
+    // Edge fluxes.
+    for (uint32_t j = tid; j < it.ne; j += TPB) {
+        const int cL = B.cl[j], cR = B.cr[j];
+        const float nx = B.nx[j], ny = B.ny[j];
+        float hL, huL, hvL, hR, huR, hvR;
+        const uint32_t lL = static_cast<uint32_t>(cL - base);
+        if (lL < static_cast<uint32_t>(kTileCells)) {
+            hL = C0[lL];
+            huL = C1[lL];
+            hvL = C2[lL];
+        } else {
+            load_state<STAGE>(s, cL, hL, huL, hvL);
+        }
+        if (cR < 0) {
+            hR = hL;
+            wall_mirror(huL, hvL, nx, ny, huR, hvR);
+        } else {
+            const uint32_t lR = static_cast<uint32_t>(cR - base);
+            if (lR < static_cast<uint32_t>(kTileCells)) {
+                hR = C0[lR];
+                huR = C1[lR];
+                hvR = C2[lR];
+            } else {
+                load_state<STAGE>(s, cR, hR, huR, hvR);
+            }
+        }
+        const bool live = !(hL < p.dry_tol && hR < p.dry_tol);
+        const float len = B.len[j], dzl = B.dzl[j], dzr = B.dzr[j];
+        live_w[j] = live ? 1 : 0;
+        if (!live) continue;
+        float w0, w1, w2, w3, w4, w5;
+        edge_words(p, cR, nx, ny, len, dzl, dzr, hL, huL, hvL, hR, huR, hvR, w0, w1, w2, w3, w4, w5);
+        W0[j] = w0;
+        W1[j] = w1;
+        W2[j] = w2;
+        W3[j] = w3;
+        W4[j] = w4;
+        if (STAGE == 1) W5[j] = __float_as_int(w5);
+    }
+    __syncthreads();
+
+    bool wet = false;
+    uint32_t bound = kNoBound;
+    if (tid < it.cells) {
+        float sdh = 0.0f, sdhu = 0.0f, sdhv = 0.0f, lam = 0.0f;
+        const uint32_t k0 = B.cptr[tid] - B.cptr[0], k1 = B.cptr[tid + 1] - B.cptr[0];
+        for (uint32_t q = k0; q < k1; ++q) {
+            const uint32_t v = B.lcsr[q];
+            const uint32_t j = v >> 1;
+            if (!live_w[j]) continue;
+            if (v & 1u) {
+                sdh -= W0[j];
+                sdhu -= W3[j];
+                sdhv -= W4[j];
+            } else {
+                sdh += W0[j];
+                sdhu += W1[j];
+                sdhv += W2[j];
+            }
+            if (STAGE == 1) lam += __int_as_float(W5[j]);
+        }
+        const float *c = B.c;
+        const float *ci = c + in_col * kTileCells, *cc = c + com_col * kTileCells;
+        update_cell<STAGE, COMP, CLAMP>(s, p, cfl, dt, base + tid, c[4 * kTileCells + tid], c[5 * kTileCells + tid],
+                                        ci[tid], ci[kTileCells + tid], ci[2 * kTileCells + tid],
+                                        ci[3 * kTileCells + tid], STAGE ? cc[tid] : 0.0f,
+                                        STAGE ? cc[kTileCells + tid] : 0.0f, STAGE ? cc[2 * kTileCells + tid] : 0.0f,
+                                        STAGE ? cc[3 * kTileCells + tid] : 0.0f, sdh, sdhu, sdhv, lam, wet, bound,
+                                        keep_pred ? B.c + 6 * kTileCells + tid : nullptr);
+    }
+    if (STAGE == 1) {
+        const int any_wet = __syncthreads_or(wet);
+        const uint32_t bmin = block_min_any(bound, red);
+        if (tid == 0) {
+            if (any_wet) s.blk[kBlkWords * b + kBlkWet] = 1u;
+            if (bmin != kNoBound) atomicMin(&s.dt_buf[kDtWords * it.inst + 1], bmin);
+            computed += it.cells;
+        }
+    }
+}
 
 // One stage over the current tile work items: items blockIdx.x, + gridDim.x, ...
 // `smem` holds the two mbarriers (initialised by the caller) and the two staged
 // buffers; `k` counts this CTA's buffer uses across calls (their mbarrier
 // phases); computed cells of the corrector accumulate in `computed`.
+// KEEP (the persistent kernel, which runs the corrector right after the
+// predictor over the same list): one buffer layout for both stages, flux words
+// in arrays of their own, and the predictor's new state kept in columns 6..9;
+// when every CTA has at most one item, the corrector then computes from the
+// predictor's staged tile without staging anything.
 // Returns false when staged data did not arrive within the wait bound (the
 // copies in flight have had one more bounded wait; the caller must stop).
-template <int STAGE, bool COMP, bool CLAMP, int TPB>
+template <int STAGE, bool COMP, bool CLAMP, int TPB, bool KEEP = false>
 __device__ bool tiled_pass(const swe_mesh_t &m, const swe_state_t &s, const Phys &p, float cfl, unsigned char *smem,
                            TiledShared<TPB> &sh, uint32_t &k, uint64_t &computed) {
-    const uint32_t count = *reinterpret_cast<volatile const uint32_t *>(s.sched + kSchedItems);
-    if (blockIdx.x >= count) return true;
-    constexpr uint32_t nc = STAGE ? 10u : 6u;
+    constexpr uint32_t nc = (STAGE || KEEP) ? 10u : 6u;
     const TilePlan L = tile_plan(m.max_sub_edges, m.max_sub_slots, nc);
+    float *F = KEEP ? reinterpret_cast<float *>(smem + L.total) : nullptr;
     uint32_t *red = sh.red;
     uint4 *items = sh.items;
     uint32_t *dts = sh.dts;
     const uint4 *work = reinterpret_cast<const uint4 *>(s.items);
     const uint32_t tid = threadIdx.x;
-    if (tid < 32u) {
-        const uint4 v = work[blockIdx.x];
-        const Item it = unpack(v);
-        if (tid == 0) {
-            items[k & 1u] = v;
-            dts[k & 1u] = s.dt_buf[kDtWords * it.inst];
-        }
-        tile_issue<STAGE>(m, s, it, tile_buf(smem, L, k & 1u));
+
+    if (KEEP && STAGE == 1 && sh.count <= gridDim.x) {
+        // The predictor's tile of this CTA is still staged (same list, one item per CTA).
+        if (blockIdx.x >= sh.count) return true;
+        const uint32_t kb = (k - 1u) & 1u;
+        const uint32_t dt_bits = dts[kb];
+        if (dt_bits != 0u)
+            tile_compute<1, COMP, CLAMP, TPB>(m, s, p, cfl, tile_buf(smem, L, kb), unpack(items[kb]),
+                                              __uint_as_float(dt_bits), 6u, 0u, F, L.capE, red, computed, false);
+        __syncthreads();
+        return true;
     }
+
+    if (tid < 32u) {
+        // The item count and this CTA's first item in one round trip (the item buffer
+        // holds four per block, so the read stays inside it even past the count).
+        uint32_t cnt = 0u;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (tid == 0) {
+            cnt = *reinterpret_cast<volatile const uint32_t *>(s.sched + kSchedItems);
+            if (blockIdx.x < 4u * m.n_blocks) v = work[blockIdx.x];
+        }
+        cnt = __shfl_sync(0xFFFFFFFFu, cnt, 0);
+        v.x = __shfl_sync(0xFFFFFFFFu, v.x, 0);
+        v.y = __shfl_sync(0xFFFFFFFFu, v.y, 0);
+        v.z = __shfl_sync(0xFFFFFFFFu, v.z, 0);
+        v.w = __shfl_sync(0xFFFFFFFFu, v.w, 0);
+        if (tid == 0) sh.count = cnt;
+        if (blockIdx.x < cnt) {
+            const Item it = unpack(v);
+            if (tid == 0) {
+                items[k & 1u] = v;
+                dts[k & 1u] = s.dt_buf[kDtWords * it.inst];
+            }
+            tile_issue<STAGE>(m, s, it, tile_buf(smem, L, k & 1u));
+        }
+    }
+    __syncthreads();
+    const uint32_t count = sh.count;
+    if (blockIdx.x >= count) return true;
+    const bool keep_pred = KEEP && STAGE == 0 && count <= gridDim.x;
 
     for (uint32_t w = blockIdx.x; w < count; w += gridDim.x, ++k) {
         const TileBuf B = tile_buf(smem, L, k & 1u);
@@ -255,102 +405,15 @@ __device__ bool tiled_pass(const swe_mesh_t &m, const swe_state_t &s, const Phys
             if (wn < count) mbar_wait(tile_buf(smem, L, (k + 1u) & 1u).bar, ((k + 1u) >> 1) & 1u);
             return false;
         }
-        const Item it = unpack(items[k & 1u]);
         const uint32_t dt_bits = dts[k & 1u];
-        if (dt_bits != 0u) {
-            const float dt = __uint_as_float(dt_bits);
-            const uint32_t b = it.tile >> 2;
-            if (STAGE == 0 && (it.tile & 3u) == 0u && tid == 0) s.blk[kBlkWords * b + kBlkWet] = 0u;
-            const float *C0 = B.c, *C1 = B.c + kTileCells, *C2 = B.c + 2 * kTileCells;
-            const int base = static_cast<int>(it.tile * kTileCells);
-
-            // Edge fluxes, written in place over the consumed records.
-            for (uint32_t j = tid; j < it.ne; j += TPB) {
-                const int cL = B.cl[j], cR = B.cr[j];
-                const float nx = B.nx[j], ny = B.ny[j];
-                float hL, huL, hvL, hR, huR, hvR;
-                const uint32_t lL = static_cast<uint32_t>(cL - base);
-                if (lL < static_cast<uint32_t>(kTileCells)) {
-                    hL = C0[lL];
-                    huL = C1[lL];
-                    hvL = C2[lL];
-                } else {
-                    load_state<STAGE>(s, cL, hL, huL, hvL);
-                }
-                if (cR < 0) {
-                    hR = hL;
-                    wall_mirror(huL, hvL, nx, ny, huR, hvR);
-                } else {
-                    const uint32_t lR = static_cast<uint32_t>(cR - base);
-                    if (lR < static_cast<uint32_t>(kTileCells)) {
-                        hR = C0[lR];
-                        huR = C1[lR];
-                        hvR = C2[lR];
-                    } else {
-                        load_state<STAGE>(s, cR, hR, huR, hvR);
-                    }
-                }
-                const bool live = !(hL < p.dry_tol && hR < p.dry_tol);
-                B.cr[j] = live ? 1 : 0;
-                if (!live) continue;
-                float w0, w1, w2, w3, w4, w5;
-                edge_words(p, cR, nx, ny, B.len[j], B.dzl[j], B.dzr[j], hL, huL, hvL, hR, huR, hvR, w0, w1, w2, w3,
-                           w4, w5);
-                B.nx[j] = w0;
-                B.ny[j] = w1;
-                B.len[j] = w2;
-                B.dzl[j] = w3;
-                B.dzr[j] = w4;
-                if (STAGE == 1) B.cl[j] = __float_as_int(w5);
-            }
-            __syncthreads();
-
-            bool wet = false;
-            uint32_t bound = kNoBound;
-            if (tid < it.cells) {
-                float sdh = 0.0f, sdhu = 0.0f, sdhv = 0.0f, lam = 0.0f;
-                const uint32_t k0 = B.cptr[tid] - B.cptr[0], k1 = B.cptr[tid + 1] - B.cptr[0];
-                for (uint32_t q = k0; q < k1; ++q) {
-                    const uint32_t v = B.lcsr[q];
-                    const uint32_t j = v >> 1;
-                    if (!B.cr[j]) continue;
-                    if (v & 1u) {
-                        sdh -= B.nx[j];
-                        sdhu -= B.dzl[j];
-                        sdhv -= B.dzr[j];
-                    } else {
-                        sdh += B.nx[j];
-                        sdhu += B.ny[j];
-                        sdhv += B.len[j];
-                    }
-                    if (STAGE == 1) lam += __int_as_float(B.cl[j]);
-                }
-                const float *c = B.c;
-                update_cell<STAGE, COMP, CLAMP>(s, p, cfl, dt, base + tid, c[4 * kTileCells + tid],
-                                                c[5 * kTileCells + tid], c[tid], c[kTileCells + tid],
-                                                c[2 * kTileCells + tid], c[3 * kTileCells + tid],
-                                                STAGE ? c[6 * kTileCells + tid] : 0.0f,
-                                                STAGE ? c[7 * kTileCells + tid] : 0.0f,
-                                                STAGE ? c[8 * kTileCells + tid] : 0.0f,
-                                                STAGE ? c[9 * kTileCells + tid] : 0.0f, sdh, sdhu, sdhv, lam, wet,
-                                                bound);
-            }
-            if (STAGE == 1) {
-                const int any_wet = __syncthreads_or(wet);
-                const uint32_t bmin = block_min_any(bound, red);
-                if (tid == 0) {
-                    if (any_wet) s.blk[kBlkWords * b + kBlkWet] = 1u;
-                    if (bmin != kNoBound) atomicMin(&s.dt_buf[kDtWords * it.inst + 1], bmin);
-                    computed += it.cells;
-                }
-            }
-        }
+        if (dt_bits != 0u)
+            tile_compute<STAGE, COMP, CLAMP, TPB>(m, s, p, cfl, B, unpack(items[k & 1u]), __uint_as_float(dt_bits), 0u,
+                                                  6u, F, L.capE, red, computed, keep_pred);
         // This buffer is refilled by bulk copies two items on.
         fence_proxy_async();
         __syncthreads();
     }
     return true;
 }
-
 
 }  // namespace swe
