@@ -35,6 +35,8 @@ constexpr int kSchedDone = 2;       // CTAs of the dilation that finished
 constexpr int kSchedItems = 3;      // tile work items of the current step
 constexpr int kSchedNextItems = 4;  // tile work items appended by the dilation
 constexpr int kSchedComputed = 6;   // [6,7]: uint64 cells computed over real steps
+constexpr int kSchedEpoch = 10;     // steps of the persistent kernel since the run's prologue
+constexpr int kSchedPrevActive = 11;  // blocks of the previous step's list (persistent kernel)
 
 // A tile work item: x = tile | (real cells << 25), y = first edge record,
 // z = first local-CSR entry, w = edge count | (padded slot count << 11) | (instance << 22).

@@ -202,8 +202,10 @@ using namespace swe;
 extern "C" {
 
 size_t swe_workspace_bytes(uint32_t n_blocks, uint32_t n_inst) {
-    return static_cast<size_t>(n_blocks) * sizeof(uint32_t)          // active_list
-           + static_cast<size_t>(n_blocks) * 4u * 4u * sizeof(uint32_t)  // items
+    return static_cast<size_t>(n_blocks) * 2u * sizeof(uint32_t)          // active_list, two halves
+           + static_cast<size_t>(n_blocks) * 2u * 4u * 4u * sizeof(uint32_t)  // items, two halves
+           + static_cast<size_t>(n_blocks) * 2u * sizeof(uint32_t)          // marks
+           + 64u * sizeof(uint32_t)                                        // sync
            + 16u * sizeof(uint32_t)                                   // sched
            + static_cast<size_t>(n_inst) * kDtWords * sizeof(uint32_t)  // dt_buf
            + static_cast<size_t>(n_inst) * sizeof(swe_ctrl_t);       // ctrl

@@ -74,44 +74,37 @@ __device__ __forceinline__ bool grid_sync(GridSync &g, int *flag, F last) {
 }
 
 // Dilation of the wet marks over each block's two-ring and compaction into the
-// next step's block list and tile work items (the dilate_compact kernel's work):
-// one warp per block, its lanes reading the two-ring in parallel, one pair of
-// atomics per active block.
-__device__ __forceinline__ void dilate_pass(const swe_mesh_t &m, const swe_state_t &s, int all_active) {
+// next step's block list and tile work items (the dilate_compact kernel's
+// work), for active_set = 0: every block of a running instance is listed.
+// One warp per block.
+__device__ __forceinline__ void dilate_all_pass(const swe_mesh_t &m, const swe_state_t &s, const Spread &sp) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     for (uint32_t b = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); b < m.n_blocks; b += warps) {
         if (s.dt_buf[kDtWords * m.block_inst[b]] == 0u) continue;  // a no-op step keeps its flags
-        uint32_t v;
-        if (all_active) {
-            v = 1u;
-        } else {
-            const uint32_t k0 = m.ring_ptr[b], k1 = m.ring_ptr[b + 1];
-            v = (lane == 0) ? (s.blk[kBlkWords * b + kBlkWet] | s.blk[kBlkWords * b + kBlkForced]) : 0u;
-            for (uint32_t k = k0 + lane; k < k1; k += 32) {
-                const uint32_t nb = m.ring_idx[k];
-                v |= s.blk[kBlkWords * nb + kBlkWet] | s.blk[kBlkWords * nb + kBlkForced];
-            }
-            v = __any_sync(0xFFFFFFFFu, v != 0u) ? 1u : 0u;
-        }
-        if (lane == 0) s.blk[kBlkWords * b + kBlkActive] = v;
-        if (!v) continue;
-        const uint32_t cells = m.block_cells[b];
-        const uint32_t n_items = (cells + kTileCells - 1) / kTileCells;
-        uint32_t pos = 0, ipos = 0;
         if (lane == 0) {
-            pos = atomicAdd(&s.sched[kSchedNext], 1u);
-            ipos = atomicAdd(&s.sched[kSchedNextItems], n_items);
+            s.blk[kBlkWords * b + kBlkActive] = 1u;
+            list_block(m, s, sp, b);
         }
-        pos = __shfl_sync(0xFFFFFFFFu, pos, 0);
-        ipos = __shfl_sync(0xFFFFFFFFu, ipos, 0);
-        if (lane == 0 && pos < m.n_blocks) s.active_list[pos] = b;
-        if (lane < n_items && ipos + lane < 4u * m.n_blocks) {
-            const uint32_t t = 4u * b + lane;
-            const uint32_t l0 = m.sub_lcsr_ptr[t];
-            reinterpret_cast<uint4 *>(s.items)[ipos + lane] =
-                make_item(t, min(static_cast<uint32_t>(kTileCells), cells - lane * kTileCells), m.sub_ptr[t], l0,
-                          m.sub_count[t], m.sub_lcsr_ptr[t + 1] - l0, m.block_inst[b]);
+    }
+}
+
+// Active flags of the step whose lists were just built by spreading: every block
+// of the current list is active; a block of the previous list that was not listed
+// again is not, unless its instance did not run the previous step (a no-op step
+// keeps its flags, as the dilation does). dt_buf[4 i + 2] holds each instance's
+// dt of the previous step. Spread over the CTAs from the last one down, which
+// are the ones without tiles when the lists are short.
+__device__ __forceinline__ void flag_pass(const swe_mesh_t &m, const swe_state_t &s, const uint32_t *cur, uint32_t n_cur,
+                                          const uint32_t *prev, uint32_t n_prev, uint32_t listed_epoch) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t t = (gridDim.x - 1u - blockIdx.x) * blockDim.x + threadIdx.x; t < n_cur + n_prev; t += stride) {
+        if (t < n_cur) {
+            s.blk[kBlkWords * cur[t] + kBlkActive] = 1u;
+        } else {
+            const uint32_t b = prev[t - n_cur];
+            if (s.marks[2u * b] != listed_epoch && s.dt_buf[kDtWords * m.block_inst[b] + 2u] != 0u)
+                s.blk[kBlkWords * b + kBlkActive] = 0u;
         }
     }
 }
@@ -123,44 +116,92 @@ __global__ void __launch_bounds__(kPersistThreads, 1024 / kPersistThreads)
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ TiledShared<kPersistThreads> sh;
     __shared__ int flag[2];
+    __shared__ uint32_t epoch0;
     GridSync g{s.sync, s.sync + 32, 0u};
     if (threadIdx.x == 0) {
         mbar_init(reinterpret_cast<uint64_t *>(smem), 1u);
         mbar_init(reinterpret_cast<uint64_t *>(smem) + 1, 1u);
         fence_barrier_init();
         g.epoch = ld_acquire_u32(g.gen);
+        epoch0 = *reinterpret_cast<volatile uint32_t *>(s.sched + kSchedEpoch);  // before any CTA's first barrier
     }
     __syncthreads();
     const uint32_t first = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    // the two halves of the lists: the step's current list in half (step & 1)
+    uint32_t *const list0 = s.active_list, *const list1 = s.active_list + m.n_blocks;
+    uint4 *const items0 = reinterpret_cast<uint4 *>(s.items), *const items1 = items0 + 4u * m.n_blocks;
+    auto lists = [&](uint32_t h) { return h ? list1 : list0; };
+    auto item_sets = [&](uint32_t h) { return h ? items1 : items0; };
     auto nothing = [] {};
-    auto control = [&] {
-        // every instance's step control, then the new lists become current
-        for (uint32_t i = threadIdx.x; i < m.n_inst; i += blockDim.x)
-            step_control(s.ctrl + i, s.dt_buf + kDtWords * i, 1);
-        if (threadIdx.x == 0) {
-            volatile uint32_t *sched = s.sched;
-            sched[kSchedActive] = sched[kSchedNext];
-            sched[kSchedItems] = sched[kSchedNextItems];
-            sched[kSchedNext] = 0u;
-            sched[kSchedNextItems] = 0u;
-        }
-    };
     uint32_t k = 0;
     uint64_t computed = 0;
     bool ok = true;
-    for (uint32_t step = 0; step < n_steps; ++step) {
-        if (!(ok = tiled_pass<0, COMP, CLAMP, kPersistThreads, true>(m, s, p, cfl, smem, sh, k, computed))) break;
-        if (!(ok = grid_sync(g, flag, nothing))) break;
-        if (!(ok = tiled_pass<1, COMP, CLAMP, kPersistThreads, true>(m, s, p, cfl, smem, sh, k, computed))) break;
-        if (!(ok = grid_sync(g, flag, nothing))) break;
-        if (src.count) {
-            source_apply(m, s, src, p.dry_tol, COMP ? 1 : 0, first, stride);
-            if (!(ok = grid_sync(g, flag, nothing))) break;
-            source_bound(m, s, src, p, cfl, first, stride);
-            if (!(ok = grid_sync(g, flag, nothing))) break;
+    uint32_t step = 0;
+    for (; step < n_steps; ++step) {
+        const uint32_t cur = step & 1u, nxt = cur ^ 1u;
+        const uint32_t epoch = epoch0 + step + 1u;
+        swe_state_t sj = s;
+        sj.active_list = lists(cur);
+        sj.items = reinterpret_cast<uint32_t *>(item_sets(cur));
+        const Spread sp{lists(nxt), item_sets(nxt), epoch};
+        const Spread none{};
+        if (!(ok = tiled_pass<0, COMP, CLAMP, kPersistThreads, true>(m, sj, p, cfl, smem, sh, k, computed))) break;
+        if (step > 0u && !all_active) {
+            const volatile uint32_t *sched = s.sched;
+            flag_pass(m, s, lists(cur), sched[kSchedActive], lists(nxt), sched[kSchedPrevActive], epoch - 1u);
         }
-        dilate_pass(m, s, all_active);
+        if (!(ok = grid_sync(g, flag, nothing))) break;
+        if (!(ok = tiled_pass<1, COMP, CLAMP, kPersistThreads, true>(m, sj, p, cfl, smem, sh, k, computed,
+                                                                      all_active ? none : sp)))
+            break;
+        if (src.count) {
+            if (!(ok = grid_sync(g, flag, nothing))) break;
+            source_apply(m, sj, src, p.dry_tol, COMP ? 1 : 0, first, stride);
+            if (!(ok = grid_sync(g, flag, nothing))) break;
+            source_bound(m, sj, src, p, cfl, first, stride);
+            if (!all_active) {
+                for (uint32_t q = first; q < src.count; q += stride) {
+                    const uint32_t b = src.cells[q] >> 8;
+                    if (s.blk[kBlkWords * b + kBlkWet] != 0u && s.dt_buf[kDtWords * m.block_inst[b]] != 0u)
+                        spread_thread(m, s, sp, b);
+                }
+            }
+        }
+        if (all_active) {
+            if (!(ok = grid_sync(g, flag, nothing))) break;
+            dilate_all_pass(m, s, sp);
+        }
+        auto control = [&] {
+            // every instance's step control (keeping the dt of the step it ends), then the new lists become current
+            for (uint32_t i = threadIdx.x; i < m.n_inst; i += blockDim.x) {
+                s.dt_buf[kDtWords * i + 2u] = s.dt_buf[kDtWords * i];
+                step_control(s.ctrl + i, s.dt_buf + kDtWords * i, 1);
+            }
+            if (threadIdx.x == 0) {
+                volatile uint32_t *sched = s.sched;
+                sched[kSchedPrevActive] = sched[kSchedActive];
+                sched[kSchedActive] = sched[kSchedNext];
+                sched[kSchedItems] = sched[kSchedNextItems];
+                sched[kSchedNext] = 0u;
+                sched[kSchedNextItems] = 0u;
+                sched[kSchedEpoch] = epoch;
+            }
+        };
         if (!(ok = grid_sync(g, flag, control))) break;
+    }
+    if (ok && step > 0u) {
+        // Hand the lists over in the first halves with their flags, as the other kernels expect them.
+        const uint32_t cur = step & 1u;
+        const volatile uint32_t *sched = s.sched;
+        const uint32_t n_cur = sched[kSchedActive], n_items = sched[kSchedItems];
+        if (!all_active) flag_pass(m, s, lists(cur), n_cur, lists(cur ^ 1u), sched[kSchedPrevActive], epoch0 + step);
+        if (cur == 1u) {
+            ok = grid_sync(g, flag, nothing);
+            if (ok) {
+                for (uint32_t i = first; i < n_cur; i += stride) list0[i] = list1[i];
+                for (uint32_t i = first; i < n_items; i += stride) items0[i] = items1[i];
+            }
+        }
     }
     if (threadIdx.x == 0) {
         if (!ok) atomicOr(&s.ctrl->error, 2u);
@@ -224,7 +265,7 @@ extern "C" int swe_steps(const swe_mesh_t *mesh, const swe_state_t *state, const
         }
         return SWE_OK;
     }
-    if (!state->sync) return SWE_ERR_ARGUMENT;
+    if (!state->sync || !state->marks) return SWE_ERR_ARGUMENT;
     if (mesh->max_sub_edges > 2047u || mesh->max_sub_slots > 2047u || mesh->n_inst > 1023u) return SWE_ERR_TOO_LARGE;
     if (sources->count && (!sources->cells || !sources->rate)) return SWE_ERR_ARGUMENT;
     if (params->compensated)

@@ -161,8 +161,9 @@ class ResidentEngine:
         n, nb, ni, dev = self.layout.n_padded_cells, self.n_blocks, self.n_inst, self.device
         self._t = {name: torch.zeros(n, dtype=torch.float32, device=dev) for name in STATE_ARRAYS}
         self._blk = torch.zeros(3 * nb, dtype=torch.int32, device=dev)
-        self._active_list = torch.zeros(nb, dtype=torch.int32, device=dev)
-        self._items = torch.zeros(16 * nb, dtype=torch.int32, device=dev)  # 4 tiles x 4 words per block
+        self._active_list = torch.zeros(2 * nb, dtype=torch.int32, device=dev)  # two halves
+        self._items = torch.zeros(32 * nb, dtype=torch.int32, device=dev)  # two halves of 4 tiles x 4 words per block
+        self._marks = torch.zeros(2 * nb, dtype=torch.int32, device=dev)  # listed / spread epochs
         self._sched = torch.zeros(8, dtype=torch.int64, device=dev)  # 16 uint32 words
         dt = np.zeros(4 * ni, np.uint32)
         dt[1::4] = np.float32(1e30).view(np.uint32)
@@ -185,6 +186,7 @@ class ResidentEngine:
         s.dt_buf = self._dt_buf.data_ptr()
         s.ctrl = self._ctrl_dev.data_ptr()
         s.sync = self._sync.data_ptr()
+        s.marks = self._marks.data_ptr()
         self._state = s
 
     def _params(self) -> native.SweParams:
@@ -358,8 +360,9 @@ class ResidentEngine:
     def _enqueue_prologue(self) -> None:
         p = self._params()
         with torch.cuda.stream(self._stream):
-            self._sched[:3].zero_()  # list counters; words 6-7 keep the computed-cells total
+            self._sched[:3].zero_()  # list counters and epoch; words 6-7 keep the computed-cells total
             self._sched[4:].zero_()
+            self._marks.zero_()
             native.check(
                 self._lib.swe_prologue(
                     ctypes.byref(self._mesh), ctypes.byref(self._state), ctypes.byref(p), self._cuda_stream

@@ -73,7 +73,7 @@ class SweState(ctypes.Structure):
         (name, _P)
         for name in (
             "h", "hu", "hv", "h_lo", "h1", "hu1", "hv1", "h1_lo", "clamp_mass", "blk", "active_list", "items",
-            "sched", "dt_buf", "ctrl", "sync",
+            "sched", "dt_buf", "ctrl", "sync", "marks",
         )
     ]
 

@@ -61,14 +61,14 @@ def test_status_strings_and_argument_checks(lib: ctypes.CDLL) -> None:
     assert lib.swe_prologue(None, None, None, None) == 1
     assert lib.swe_step_control(None, None, 1, 0, None) == 1
     assert lib.swe_volume_fp64(None, None, None, 0, None, None, None) == 1
-    assert lib.swe_workspace_bytes(3907, 1) >= 3907 * 4 * 17 + 64 + 16 + 48
+    assert lib.swe_workspace_bytes(3907, 1) >= 3907 * 4 * 36 + 64 + 256 + 16 + 48
     assert lib.swe_workspace_bytes(3907, 64) == lib.swe_workspace_bytes(3907, 1) + 63 * (16 + 48)
     assert lib.swe_configure(None, 0, None) == 1
 
 
 def test_ctypes_structs_match_the_header_layout() -> None:
     assert ctypes.sizeof(native.SweMesh) == 16 + 17 * 8 + 8 + 11 * 8
-    assert ctypes.sizeof(native.SweState) == 16 * 8
+    assert ctypes.sizeof(native.SweState) == 17 * 8
     assert ctypes.sizeof(native.SweParams) == 32
     assert ctypes.sizeof(native.SweSources) == 7 * 8 + 8
 
