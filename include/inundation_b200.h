@@ -252,6 +252,8 @@ typedef struct {
     float *gn;                  /* d loss / d Manning n, per cell (accumulated) */
     float *gz;                  /* d loss / d bed elevation, per cell (accumulated) */
     double *gq;                 /* d loss / d knot discharge, per knot of swe_sources_t (accumulated) */
+    uint32_t *sync;             /* NULL: one launch per phase; else 64 zeroed words for the grid barrier of a
+                                   single cooperative launch per segment (word 40 set: a barrier wait timed out) */
     float cut_depth;            /* no derivative flows through a cell or face depth below this (0: the
                                    exact derivative of the discrete step) */
 } swe_adjoint_t;
@@ -271,7 +273,7 @@ typedef struct {
 int swe_bed_steps(const swe_mesh_t *mesh, const float *z, float *tile_dzl, float *tile_dzr, uint32_t tile_records,
                   float *sub_dzl, float *sub_dzr, uint32_t sub_records, swe_stream_t stream);
 
-/* swe_stage with 256-cell blocks that also stores every computed cell's gathered sums. */
+/* swe_stage (kernel 0 or 1) that also stores every computed cell's gathered sums. */
 int swe_stage_taped(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params_t *params, int stage,
                     float *sums, swe_stream_t stream);
 

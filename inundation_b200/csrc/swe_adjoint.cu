@@ -27,7 +27,7 @@
 
 #include <cstdint>
 
-#include "swe_common.cuh"
+#include "swe_grid.cuh"
 
 namespace swe {
 
@@ -373,8 +373,8 @@ __device__ __forceinline__ Slot slot_of(const swe_tape_t &T, uint32_t k, uint32_
 }
 
 // The misfit's gradient at the state after the step, then the hydrograph knots' gradients.
-__global__ void adj_boundary_kernel(swe_tape_t T, swe_adjoint_t a, swe_sources_t src, swe_gauges_t gg, uint32_t k,
-                                    uint32_t n, uint32_t row) {
+__device__ void adj_boundary(const swe_tape_t &T, const swe_adjoint_t &a, const swe_sources_t &src,
+                             const swe_gauges_t &gg, uint32_t k, uint32_t n, uint32_t row) {
     const float *h1 = T.h + static_cast<size_t>(k + 1) * n, *lo1 = T.h_lo + static_cast<size_t>(k + 1) * n;
     if (gg.count && row < gg.steps) {
         const float *obs = gg.obs + static_cast<size_t>(row) * gg.count;
@@ -409,8 +409,8 @@ __global__ void adj_boundary_kernel(swe_tape_t T, swe_adjoint_t a, swe_sources_t
 
 // The Heun average and the corrector's cell update, reversed; also the
 // predictor state (recomputed) and the block marks of this step.
-__global__ void __launch_bounds__(kThreads)
-    adj_cell1_kernel(swe_mesh_t m, swe_tape_t T, swe_adjoint_t a, Phys p, uint32_t k, uint32_t tag) {
+__device__ void adj_cell1(const swe_mesh_t &m, const swe_tape_t &T, const swe_adjoint_t &a, const Phys &p, uint32_t k,
+                          uint32_t tag) {
     const uint32_t n = m.n_blocks * kBlockCells;
     const uint32_t count = T.count[k];
     const Slot S = slot_of(T, k, n, m.n_blocks);
@@ -452,8 +452,7 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // The predictor's cell update, reversed.
-__global__ void __launch_bounds__(kThreads)
-    adj_cell0_kernel(swe_mesh_t m, swe_tape_t T, swe_adjoint_t a, Phys p, uint32_t k) {
+__device__ void adj_cell0(const swe_mesh_t &m, const swe_tape_t &T, const swe_adjoint_t &a, const Phys &p, uint32_t k) {
     const uint32_t n = m.n_blocks * kBlockCells;
     const uint32_t count = T.count[k];
     const Slot S = slot_of(T, k, n, m.n_blocks);
@@ -483,21 +482,23 @@ __global__ void __launch_bounds__(kThreads)
 // the start state elsewhere; adds into the predictor's adjoint). STAGE 0: the
 // predictor (inputs: the start state; adds into the start state's adjoint).
 template <int STAGE>
-__global__ void __launch_bounds__(kThreads)
-    adj_edge_kernel(swe_mesh_t m, swe_tape_t T, swe_adjoint_t a, Phys p, uint32_t k, uint32_t tag) {
-    extern __shared__ float4 smem4[];
+__device__ void adj_edge(const swe_mesh_t &m, const swe_tape_t &T, const swe_adjoint_t &a, const Phys &p, uint32_t k,
+                         uint32_t tag, float *G) {
     const uint32_t count = T.count[k];
-    float *G = reinterpret_cast<float *>(smem4);
-    const uint32_t cap = (m.max_tile_edges + 3u) & ~3u;
+    const uint32_t cap = (m.max_sub_edges + 3u) & ~3u;
     const uint32_t n = m.n_blocks * kBlockCells;
     const Slot S = slot_of(T, k, n, m.n_blocks);
-    for (uint32_t w = blockIdx.x; w < count; w += gridDim.x) {
-        const uint32_t b = S.list[w];
-        const uint32_t base = m.tile_ptr[b], ne = m.tile_count[b];
+    // one 64-cell tile per CTA pass: four per active block, one edge record per thread
+    for (uint32_t w = blockIdx.x; w < 4u * count; w += gridDim.x) {
+        const uint32_t b = S.list[w >> 2], q4 = w & 3u;
+        const uint32_t cells = m.block_cells[b];
+        if (q4 * kTileCells >= cells) continue;
+        const uint32_t t = 4u * b + q4;
+        const uint32_t base = m.sub_ptr[t], ne = m.sub_count[t];
         for (uint32_t j = threadIdx.x; j < ne; j += kThreads) {
             const uint32_t e = base + j;
-            const int cL = m.tile_cl[e], cR = m.tile_cr[e];
-            const float nx = m.tile_nx[e], ny = m.tile_ny[e];
+            const int cL = m.sub_cl[e], cR = m.sub_cr[e];
+            const float nx = m.sub_nx[e], ny = m.sub_ny[e];
             const bool actL = a.mark[static_cast<uint32_t>(cL) >> 8] == tag;
             float hL, huL, hvL, hR = 0.0f, huR = 0.0f, hvR = 0.0f;
             if (STAGE == 1 && actL) {
@@ -531,10 +532,10 @@ __global__ void __launch_bounds__(kThreads)
                             lvL = actL ? a.ls[2 * n + cL] : 0.0f;
                 const float lhR = actR ? a.ls[cR] : 0.0f, luR = actR ? a.ls[n + cR] : 0.0f,
                             lvR = actR ? a.ls[2 * n + cR] : 0.0f;
-                eg = edge_words_rev(p, cR < 0, nx, ny, m.tile_len[e], m.tile_dzl[e], m.tile_dzr[e], hL, huL, hvL, hR,
+                eg = edge_words_rev(p, cR < 0, nx, ny, m.sub_len[e], m.sub_dzl[e], m.sub_dzr[e], hL, huL, hvL, hR,
                                     huR, hvR, lhL - lhR, luL, lvL, -luR, -lvR, a.cut_depth);
             }
-            const bool face_left = m.tile_dzl[e] == 0.0f;  // the face sits on the left bed
+            const bool face_left = m.sub_dzl[e] == 0.0f;  // the face sits on the left bed
             G[j] = eg.hL;
             G[cap + j] = eg.huL;
             G[2 * cap + j] = eg.hvL;
@@ -545,11 +546,12 @@ __global__ void __launch_bounds__(kThreads)
             G[7 * cap + j] = face_left ? -eg.dzR : eg.dzL;  // d loss / d zR
         }
         __syncthreads();
-        if (threadIdx.x < m.block_cells[b]) {
-            const uint32_t i = b * kBlockCells + threadIdx.x;
+        if (threadIdx.x < min(static_cast<uint32_t>(kTileCells), cells - q4 * kTileCells)) {
+            const uint32_t i = t * kTileCells + threadIdx.x;
+            const uint32_t l0 = m.sub_lcsr_ptr[t], c0 = m.cptr[t * kTileCells];
             float sh = 0.0f, su = 0.0f, sv = 0.0f, sz = 0.0f;
             for (uint32_t q = m.cptr[i], q1 = m.cptr[i + 1]; q < q1; ++q) {
-                const uint32_t v = m.lcsr[q];
+                const uint32_t v = m.sub_lcsr[l0 + q - c0];
                 const uint32_t j = v >> 1;
                 if (v & 1u) {
                     sh += G[3 * cap + j];
@@ -576,6 +578,58 @@ __global__ void __launch_bounds__(kThreads)
         }
         __syncthreads();
     }
+}
+
+__global__ void adj_boundary_kernel(swe_tape_t T, swe_adjoint_t a, swe_sources_t src, swe_gauges_t gg, uint32_t k,
+                                    uint32_t n, uint32_t row) {
+    adj_boundary(T, a, src, gg, k, n, row);
+}
+
+__global__ void __launch_bounds__(kThreads)
+    adj_cell1_kernel(swe_mesh_t m, swe_tape_t T, swe_adjoint_t a, Phys p, uint32_t k, uint32_t tag) {
+    adj_cell1(m, T, a, p, k, tag);
+}
+
+__global__ void __launch_bounds__(kThreads) adj_cell0_kernel(swe_mesh_t m, swe_tape_t T, swe_adjoint_t a, Phys p, uint32_t k) {
+    adj_cell0(m, T, a, p, k);
+}
+
+template <int STAGE>
+__global__ void __launch_bounds__(kThreads)
+    adj_edge_kernel(swe_mesh_t m, swe_tape_t T, swe_adjoint_t a, Phys p, uint32_t k, uint32_t tag) {
+    extern __shared__ float4 smem4[];
+    adj_edge<STAGE>(m, T, a, p, k, tag, reinterpret_cast<float *>(smem4));
+}
+
+// The reverse of a whole segment in one cooperative launch: the five phases of
+// every step, slot by slot from the last, separated by grid barriers instead of
+// kernel boundaries. A barrier wait past its bound sets a.sync[40] and stops.
+__global__ void __launch_bounds__(kThreads)
+    adj_persistent_kernel(swe_mesh_t m, swe_tape_t T, swe_adjoint_t a, swe_sources_t src, swe_gauges_t gg, Phys p,
+                          uint32_t slots, uint32_t row0, uint32_t tag0) {
+    extern __shared__ float4 smem4[];
+    float *G = reinterpret_cast<float *>(smem4);
+    __shared__ int flag[2];
+    GridSync g{a.sync, a.sync + 32, 0u};
+    if (threadIdx.x == 0) g.epoch = ld_acquire_u32(g.gen);
+    __syncthreads();
+    const uint32_t n = m.n_blocks * kBlockCells;
+    auto nothing = [] {};
+    bool ok = true;
+    for (uint32_t kk = slots; kk-- > 0 && ok;) {
+        const uint32_t tag = tag0 + kk + 1;
+        if (blockIdx.x == 0) adj_boundary(T, a, src, gg, kk, n, row0 + kk);
+        if (!(ok = grid_sync(g, flag, nothing))) break;
+        adj_cell1(m, T, a, p, kk, tag);
+        if (!(ok = grid_sync(g, flag, nothing))) break;
+        adj_edge<1>(m, T, a, p, kk, tag, G);
+        if (!(ok = grid_sync(g, flag, nothing))) break;
+        adj_cell0(m, T, a, p, kk);
+        if (!(ok = grid_sync(g, flag, nothing))) break;
+        adj_edge<0>(m, T, a, p, kk, tag, G);
+        ok = grid_sync(g, flag, nothing);
+    }
+    if (!ok && threadIdx.x == 0) atomicOr(a.sync + 40, 1u);
 }
 
 // Tape record at the start of a step (or the end state at slot == capacity).
@@ -639,7 +693,7 @@ __global__ void bed_steps_kernel(const int32_t *cl, const int32_t *cr, const flo
     }
 }
 
-inline size_t edge_adj_smem(uint32_t max_tile_edges) { return ((max_tile_edges + 3u) & ~3u) * 8 * sizeof(float); }
+inline size_t edge_adj_smem(uint32_t max_sub_edges) { return ((max_sub_edges + 3u) & ~3u) * 8 * sizeof(float); }
 
 }  // namespace swe
 
@@ -685,12 +739,36 @@ int swe_adjoint_segment(const swe_mesh_t *mesh, const swe_params_t *params, cons
     if (!mesh_ok(mesh) || !params || !tape || !adj || !sources || !gauges || slots > tape->capacity ||
         mesh->n_inst != 1u || !params->compensated)
         return SWE_ERR_ARGUMENT;
-    const size_t bytes = edge_adj_smem(mesh->max_tile_edges);
+    const size_t bytes = edge_adj_smem(mesh->max_sub_edges);
     int rc = set_smem(adj_edge_kernel<0>, bytes);
     if (!rc) rc = set_smem(adj_edge_kernel<1>, bytes);
     if (rc) return rc;
     const Phys ph{params->g, params->dry_tol};
     const uint32_t n = mesh->n_blocks * kBlockCells;
+    if (adj->sync) {
+        auto kern = adj_persistent_kernel;
+        if ((rc = set_smem(kern, bytes))) return rc;
+        int per_sm = 0, dev = 0, sms = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, bytes) != cudaSuccess)
+            return SWE_ERR_CUDA;
+        if (per_sm < 1) return SWE_ERR_TOO_LARGE;
+        const uint32_t fit = static_cast<uint32_t>(per_sm) * static_cast<uint32_t>(sms);
+        const uint32_t pgrid = (params->grid == 0u || params->grid > fit) ? fit : params->grid;
+        swe_mesh_t mm = *mesh;
+        swe_tape_t tt = *tape;
+        swe_adjoint_t aa = *adj;
+        swe_sources_t sc = *sources;
+        swe_gauges_t gg = *gauges;
+        Phys ph{params->g, params->dry_tol};
+        uint32_t sl = slots, r0 = row0, t0 = tag0;
+        void *args[] = {&mm, &tt, &aa, &sc, &gg, &ph, &sl, &r0, &t0};
+        if (cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(kern), dim3(pgrid), dim3(kThreads), args, bytes,
+                                        stream) != cudaSuccess)
+            return SWE_ERR_CUDA;
+        return SWE_OK;
+    }
     // Every kernel takes the slot's active count from the tape (device memory) and
     // strides over that many list entries with a persistent grid.
     const uint32_t grid = (params->grid == 0u || params->grid > mesh->n_blocks) ? mesh->n_blocks : params->grid;

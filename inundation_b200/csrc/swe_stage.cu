@@ -140,7 +140,8 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 template <int STAGE, bool COMP, bool CLAMP>
-__global__ void __launch_bounds__(kTileThreads, 8) stage_tiled_kernel(swe_mesh_t m, swe_state_t s, Phys p, float cfl) {
+__global__ void __launch_bounds__(kTileThreads, 8)
+    stage_tiled_kernel(swe_mesh_t m, swe_state_t s, Phys p, float cfl, float *sums) {
     if (blockIdx.x >= s.sched[kSchedItems]) return;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ TiledShared<kTileThreads> sh;
@@ -152,7 +153,7 @@ __global__ void __launch_bounds__(kTileThreads, 8) stage_tiled_kernel(swe_mesh_t
     __syncthreads();
     uint32_t k = 0;
     uint64_t computed = 0;
-    if (!tiled_pass<STAGE, COMP, CLAMP, kTileThreads>(m, s, p, cfl, smem, sh, k, computed)) return;
+    if (!tiled_pass<STAGE, COMP, CLAMP, kTileThreads>(m, s, p, cfl, smem, sh, k, computed, Spread{}, sums)) return;
     if (STAGE == 1 && threadIdx.x == 0 && computed)
         atomicAdd(reinterpret_cast<unsigned long long *>(s.sched + kSchedComputed), computed);
 }
@@ -164,7 +165,7 @@ template <int STAGE, bool COMP, bool CLAMP>
 int launch_stage(const swe_mesh_t *m, const swe_state_t *s, const swe_params_t *p, cudaStream_t st,
                  float *sums = nullptr) {
     const Phys ph{p->g, p->dry_tol};
-    if (p->kernel == 1u || sums) {
+    if (p->kernel == 1u) {
         auto kern = stage_block_kernel<STAGE, COMP, CLAMP>;
         const size_t bytes = block_smem_bytes(m->max_tile_edges);
         int rc = set_smem(kern, bytes);
@@ -177,7 +178,7 @@ int launch_stage(const swe_mesh_t *m, const swe_state_t *s, const swe_params_t *
     const size_t bytes = tile_plan(m->max_sub_edges, m->max_sub_slots, STAGE ? 10u : 6u).total;
     int rc = set_smem(kern, bytes);
     if (rc) return rc;
-    kern<<<p->grid ? p->grid : 148u * 8u, kTileThreads, bytes, st>>>(*m, *s, ph, p->cfl);
+    kern<<<p->grid ? p->grid : 148u * 8u, kTileThreads, bytes, st>>>(*m, *s, ph, p->cfl, sums);
     return check_launch();
 }
 

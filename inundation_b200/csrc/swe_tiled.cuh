@@ -288,7 +288,8 @@ template <int STAGE, bool COMP, bool CLAMP, int TPB>
 __device__ __forceinline__ void tile_compute(const swe_mesh_t &m, const swe_state_t &s, const Phys &p, float cfl,
                                              const TileBuf &B, const Item &it, float dt, uint32_t in_col,
                                              uint32_t com_col, float *F, uint32_t capE, uint32_t *red,
-                                             uint64_t &computed, bool keep_pred, const Spread &sp) {
+                                             uint64_t &computed, bool keep_pred, const Spread &sp,
+                                             float *sums = nullptr) {
     const uint32_t tid = threadIdx.x;
     const uint32_t b = it.tile >> 2;
     if (STAGE == 0 && (it.tile & 3u) == 0u && tid == 0) s.blk[kBlkWords * b + kBlkWet] = 0u;
@@ -360,6 +361,12 @@ __device__ __forceinline__ void tile_compute(const swe_mesh_t &m, const swe_stat
             }
             if (STAGE == 1) lam += __int_as_float(W5[j]);
         }
+        if (sums) {  // the record the adjoint reverses
+            const uint32_t n = m.n_blocks * kBlockCells, i = base + tid;
+            sums[i] = sdh;
+            sums[n + i] = sdhu;
+            sums[2 * n + i] = sdhv;
+        }
         const float *c = B.c;
         const float *ci = c + in_col * kTileCells, *cc = c + com_col * kTileCells;
         update_cell<STAGE, COMP, CLAMP>(s, p, cfl, dt, base + tid, c[4 * kTileCells + tid], c[5 * kTileCells + tid],
@@ -394,7 +401,8 @@ __device__ __forceinline__ void tile_compute(const swe_mesh_t &m, const swe_stat
 // copies in flight have had one more bounded wait; the caller must stop).
 template <int STAGE, bool COMP, bool CLAMP, int TPB, bool KEEP = false>
 __device__ bool tiled_pass(const swe_mesh_t &m, const swe_state_t &s, const Phys &p, float cfl, unsigned char *smem,
-                           TiledShared<TPB> &sh, uint32_t &k, uint64_t &computed, const Spread &sp = Spread{}) {
+                           TiledShared<TPB> &sh, uint32_t &k, uint64_t &computed, const Spread &sp = Spread{},
+                           float *sums = nullptr) {
     constexpr uint32_t nc = (STAGE || KEEP) ? 10u : 6u;
     const TilePlan L = tile_plan(m.max_sub_edges, m.max_sub_slots, nc);
     float *F = KEEP ? reinterpret_cast<float *>(smem + L.total) : nullptr;
@@ -411,7 +419,7 @@ __device__ bool tiled_pass(const swe_mesh_t &m, const swe_state_t &s, const Phys
         const uint32_t dt_bits = dts[kb];
         if (dt_bits != 0u)
             tile_compute<1, COMP, CLAMP, TPB>(m, s, p, cfl, tile_buf(smem, L, kb), unpack(items[kb]),
-                                              __uint_as_float(dt_bits), 6u, 0u, F, L.capE, red, computed, false, sp);
+                                              __uint_as_float(dt_bits), 6u, 0u, F, L.capE, red, computed, false, sp, sums);
         __syncthreads();
         return true;
     }
@@ -469,7 +477,7 @@ __device__ bool tiled_pass(const swe_mesh_t &m, const swe_state_t &s, const Phys
         const uint32_t dt_bits = dts[k & 1u];
         if (dt_bits != 0u)
             tile_compute<STAGE, COMP, CLAMP, TPB>(m, s, p, cfl, B, unpack(items[k & 1u]), __uint_as_float(dt_bits), 0u,
-                                                  6u, F, L.capE, red, computed, keep_pred, sp);
+                                                  6u, F, L.capE, red, computed, keep_pred, sp, sums);
         // This buffer is refilled by bulk copies two items on.
         fence_proxy_async();
         __syncthreads();

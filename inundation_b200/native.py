@@ -109,7 +109,7 @@ class SweTape(ctypes.Structure):
 class SweAdjoint(ctypes.Structure):
     _fields_ = [
         *[(name, _P) for name in (
-            "lh", "lhu", "lhv", "ls", "lsh", "lshu", "lshv", "uh", "ulo", "uhu", "uhv", "mark", "gn", "gz", "gq",
+            "lh", "lhu", "lhv", "ls", "lsh", "lshu", "lshv", "uh", "ulo", "uhu", "uhv", "mark", "gn", "gz", "gq", "sync",
         )],
         ("cut_depth", ctypes.c_float),
     ]

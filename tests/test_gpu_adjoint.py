@@ -240,3 +240,18 @@ def test_gradient_with_a_film_depth_cut_matches_float64_autograd_with_the_same_c
     errs = {"n": rel(gn, gn64), "z": rel(gz, gz64), "q": rel(gq, gq64)}
     assert np.isfinite(gn).all() and np.isfinite(gz).all()
     assert max(errs.values()) <= tol, errs
+
+
+def test_one_launch_and_per_phase_reverse_agree_bit_for_bit(case) -> None:
+    """The reverse pass as one cooperative launch per segment and as one launch per phase and step."""
+    from inundation_b200.adjoint import GaugeCalibration
+
+    sc = case["sc"]
+    other = GaugeCalibration(sc.geom, sc.h0, sc.hu0, sc.hv0, gauges=sc.meta["gauges"], steps=STEPS,
+                             hydrographs=sc.hydrographs, checkpoint_every=50, dt_max=1.0, dt_init=0.05)
+    assert not case["prob"].persistent_reverse
+    other.persistent_reverse = True
+    other.set_observations(case["obs"])
+    other.loss(case["n"], case["z"], case["q"])
+    for a, b in zip(other.gradient(), case["grads"], strict=True):
+        np.testing.assert_array_equal(a, b)
