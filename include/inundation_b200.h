@@ -101,6 +101,13 @@ typedef struct {
     const uint32_t *sub_count;    /* n_blocks * 4 */
     const uint16_t *sub_lcsr;
     const uint32_t *sub_lcsr_ptr; /* n_blocks * 4 + 1 */
+    /* Open boundary edges (inundation/vulkan/solver.py:239-243, shaders/flux.py:187-294):
+       an edge with right cell -2 - k is open edge k; -1 stays a wall. open_cond holds
+       two words per open edge, its condition (0 wall, 1 free outflow, 2 normal depth,
+       3 stage, 4 inflow) and its value as float bits (sqrt(S)/n, the depth over the
+       cell's bed, or the discharge per unit width). NULL when n_open is 0. */
+    uint32_t n_open;
+    const uint32_t *open_cond;
 } swe_mesh_t;
 
 /* Mutable state and the run workspace (device pointers). */
@@ -123,6 +130,11 @@ typedef struct {
     uint32_t *sync;                /* 64 zeroed words: the grid barrier of the persistent kernel (kernel 2) */
     uint32_t *marks;               /* 2 words per block, zeroed with sched word 10 at the start of a run: the
                                       epochs at which a block was listed and its two-ring spread (kernel 2) */
+    float *open_vol;               /* 4 words per open edge, zeroed at the start of a run: the volume that
+                                      left (hi, lo) and entered (hi, lo) the mesh through it, as exact
+                                      float pairs (the per-edge form of TALLY_RESIDENT_GLSL,
+                                      inundation/vulkan/shaders/resident.py:617-660); NULL when
+                                      the mesh has no open edges */
 } swe_state_t;
 
 typedef struct {
@@ -228,7 +240,9 @@ int swe_step(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params_
    discharge knots of the inflow hydrographs, with every step's dt held at
    its forward value. A run keeps checkpoints; each segment of steps is run
    again with swe_tape_record + swe_stage_taped to fill the tape, then
-   reversed one step at a time by swe_adjoint_step (single-instance meshes). */
+   reversed one step at a time by swe_adjoint_step (single-instance meshes
+   without open edges: swe_stage_taped and swe_adjoint_segment refuse a mesh
+   whose n_open is not 0). */
 
 /* The record of a segment of steps (device pointers; slot k = k-th step of
    the segment, n = n_blocks * 256 padded cells). */
@@ -319,6 +333,14 @@ int swe_volume_fp64_noalloc(const float *h, const float *h_lo, const float *area
    reference's fast-math guard (inundation/vulkan/solver.py:449-467,
    resident.py:889-907). */
 int swe_eft_probe(float *v, swe_stream_t stream);
+
+/* The state beyond n open edges and their mass flux, on the device: case k is
+   cases[6k..6k+5] = (h, hu, hv, nx, ny, HLLC mass flux) of the cell inside, with the
+   condition words cond[2k], cond[2k+1] (kind, value bits); results[4k..4k+3] = (h, hu,
+   hv) of the ghost and the boundary mass flux. The device half of the reference's
+   probe (tests/unit/test_gpu_open_ghost.py:45-71 over shaders/flux.py:211-281). */
+int swe_open_ghost_probe(const float *cases, const uint32_t *cond, float *results, uint32_t n, float g,
+                         float dry_tol, swe_stream_t stream);
 
 /* (x^(4/3)) of n values on the device, the Manning depth power the update uses. */
 int swe_pow43(const float *x, float *out, uint32_t n, swe_stream_t stream);

@@ -9,6 +9,14 @@ count of 2^-20 s ticks, each output window runs whole submits of
 ``steps_per_graph`` steps (no-op steps past the window's stop do nothing) and
 the host reads the 48-byte control block after each submit.
 
+Open boundaries (``open_edges``, ``set_open_conditions``,
+``download_open_volumes``, ``open_volume_snapshots``) follow the reference's
+base solver and resident backend (``solver.py:140-165, 236-243, 427-440``,
+``gpu_resident_batch.py:447-466``): open edge ``k`` (stretch order) has right
+cell ``-2 - k``, every other boundary edge stays a wall, and the volume through
+each edge is kept as exact float pairs on the device and summed per stretch in
+float64 on the host.
+
 B200 specifics: a submit is one replay of a CUDA graph of ``steps_per_graph``
 steps; torch CUDA tensors own all device memory; the C ABI kernels borrow
 their pointers. There is no CPU fallback: without a GPU and the built
@@ -17,6 +25,7 @@ library, construction raises.
 
 from __future__ import annotations
 
+import dataclasses
 import math
 import sys
 import time as _time
@@ -70,13 +79,21 @@ class SWESolverB200Resident(ResidentEngine):
         del spv  # no shader binaries: the kernels are in the CUDA library
         if workgroup_size != ACTIVE_BLOCK_CELLS:
             raise ValueError(f"{B200_BACKEND} needs workgroup_size={ACTIVE_BLOCK_CELLS}, got {workgroup_size}")
-        if any(np.asarray(e).size for e in open_edges):
-            raise ValueError(f"{B200_BACKEND} does not support open boundaries yet")
         self.geom = geom
         self.N, self.E = int(geom.N), int(geom.E)
         self.steps_total = 0
+        self._open_stretches = [np.asarray(edges, dtype=np.int64).ravel() for edges in open_edges]
+        # (stretches, 2) volume out of and into the mesh at every snapshot of a run.
         self.open_volume_snapshots: list[NDArray[np.float64]] = []
-        self.n_open = 0
+        open_ids = np.concatenate([np.empty(0, dtype=np.int64), *self._open_stretches])
+        if open_ids.size:
+            if open_ids.min() < 0 or open_ids.max() >= self.E:
+                raise ValueError(f"open edges must index the mesh's {self.E} edges")
+            if np.unique(open_ids).size != open_ids.size:
+                raise ValueError("an edge is open more than once")
+            if (geom.edge_cellR[open_ids] != -1).any():
+                raise ValueError("open edges must be boundary edges (right cell -1)")
+        self._open_cells = geom.edge_cellL[open_ids].astype(np.int64)
         self._h0 = np.asarray(h0, np.float32).ravel().copy()
         self._hu0 = np.asarray(hu0, np.float32).ravel().copy()
         self._hv0 = np.asarray(hv0, np.float32).ravel().copy()
@@ -86,7 +103,9 @@ class SWESolverB200Resident(ResidentEngine):
         n0 = np.asarray(n0, np.float32).ravel()
         if n0.size != self.N:
             raise ValueError(f"n0 has {n0.size} values for {self.N} cells")
-        layout = build_tile_layout(geom)
+        cell_r = np.asarray(geom.edge_cellR).copy()
+        cell_r[open_ids] = -2 - np.arange(open_ids.size, dtype=cell_r.dtype)
+        layout = build_tile_layout(dataclasses.replace(geom, edge_cellR=cell_r) if open_ids.size else geom)
         n_pad = np.concatenate([n0, np.full(layout.n_padded_cells - self.N, 0.03, np.float32)])
         self._init_engine(layout, n_pad, g=g, dry_tol=dry_tol, cfl=cfl, device=device)
         self.reset(self._h0, self._hu0, self._hv0)
@@ -137,16 +156,34 @@ class SWESolverB200Resident(ResidentEngine):
             self._t["hv"][: self.N].copy_(torch.from_numpy(self._hv0))
             self._t["h_lo"].zero_()
             self._t["h1_lo"].zero_()
+            self._open_vol.zero_()
         self._stream.synchronize()
 
     def _reset_to_initial(self) -> None:
         self.reset(self._h0, self._hu0, self._hv0)
 
     def set_open_conditions(self, kinds: NDArray[np.uint32], values: NDArray[np.float32]) -> None:
-        raise ValueError(f"{B200_BACKEND} does not support open boundaries yet")
+        """Set every open edge's condition (``OPEN_*``), in stretch order, before a run or a phase.
+
+        A block with an edge that can bring water in from outside stays active
+        for as long as these conditions hold.
+        """
+        kinds, values = np.asarray(kinds), np.asarray(values)
+        if kinds.size != self.n_open or values.size != self.n_open:
+            raise ValueError(
+                f"expected {self.n_open} open edges, got {kinds.size} kinds and {values.size} values"
+            )
+        self.set_open_edge_conditions(kinds, values)
 
     def download_open_volumes(self) -> NDArray[np.float64]:
-        return np.zeros((0, 2), dtype=np.float64)
+        """``(stretches, 2)`` volume [m^3] out of and into the mesh since the start."""
+        per_edge = self.download_open_edge_volumes()
+        out = np.zeros((len(self._open_stretches), 2), dtype=np.float64)
+        first = 0
+        for s, edges in enumerate(self._open_stretches):
+            out[s] = per_edge[first : first + edges.size].sum(axis=0)
+            first += edges.size
+        return out
 
     def _set_sources(self, source_rate: NDArray[np.float32] | None) -> None:
         """The reference's ``_set_sources`` (gpu_resident_batch.py:529-560): nonzero cells as (cell, rate / area)."""
@@ -201,6 +238,8 @@ class SWESolverB200Resident(ResidentEngine):
             if capture_momentum_snapshots:
                 hu_snaps.append(self.download_hu())
                 hv_snaps.append(self.download_hv())
+            if self.n_open:
+                self.open_volume_snapshots.append(self.download_open_volumes())
 
         capture()
         ctrl = self._ctrl

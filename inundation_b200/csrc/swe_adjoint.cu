@@ -737,7 +737,7 @@ int swe_adjoint_segment(const swe_mesh_t *mesh, const swe_params_t *params, cons
                         const swe_adjoint_t *adj, const swe_sources_t *sources, const swe_gauges_t *gauges,
                         uint32_t slots, uint32_t row0, uint32_t tag0, swe_stream_t stream) {
     if (!mesh_ok(mesh) || !params || !tape || !adj || !sources || !gauges || slots > tape->capacity ||
-        mesh->n_inst != 1u || !params->compensated)
+        mesh->n_inst != 1u || !params->compensated || mesh->n_open)
         return SWE_ERR_ARGUMENT;
     const size_t bytes = edge_adj_smem(mesh->max_sub_edges);
     int rc = set_smem(adj_edge_kernel<0>, bytes);

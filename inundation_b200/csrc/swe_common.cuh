@@ -162,6 +162,38 @@ __device__ __forceinline__ void step_control(swe_ctrl_t *c, uint32_t *dt_buf, in
     dt_buf[1] = __float_as_uint(kDtSentinel);
 }
 
+// The state beyond boundary edge cR < 0 from the cell inside it: a wall's
+// mirror (cR == -1), or open edge -2 - cR's ghost under its condition, which
+// comes back in kind/value (resident.py:127-145). kind/value stay wall/0 for a
+// wall, so open_forced(kind, value) is the edge's forced liveness either way.
+__device__ __forceinline__ void boundary_state(const swe_mesh_t &m, const Phys &p, int cR, float hL, float huL,
+                                               float hvL, float nx, float ny, float &hR, float &huR, float &hvR,
+                                               uint32_t &kind, float &value) {
+    if (cR == -1) {
+        hR = hL;
+        wall_mirror(huL, hvL, nx, ny, huR, hvR);
+        return;
+    }
+    const uint32_t k = static_cast<uint32_t>(-2 - cR);
+    kind = m.open_cond[2u * k];
+    value = __uint_as_float(m.open_cond[2u * k + 1u]);
+    ghost_state(p, kind, value, hL, huL, hvL, nx, ny, hR, huR, hvR);
+}
+
+// Adds one stage's volume through open edge k to its out (v >= 0) or in
+// (v < 0) pair: two-sum of |v| into the high word, the old low word folded
+// into the error (resident.py:617-660, per edge). Only the thread computing
+// the edge touches its words within a stage.
+__device__ __forceinline__ void tally_open(float *vol, uint32_t k, float v) {
+    float *t = vol + 4u * k + (v < 0.0f ? 2u : 0u);
+    float sm, err, hi, lo;
+    two_sum(t[0], fabsf(v), sm, err);
+    err += t[1];
+    two_sum(sm, err, hi, lo);
+    t[0] = hi;
+    t[1] = lo;
+}
+
 // -- host helpers --------------------------------------------------------------------------------
 inline int check_launch() { return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ERR_CUDA; }
 
@@ -179,8 +211,11 @@ inline bool mesh_ok(const swe_mesh_t *m) {
            m->tile_len && m->tile_dzl && m->tile_dzr && m->tile_ptr && m->tile_count && m->cptr && m->lcsr &&
            m->area && m->n_mann && m->ring_ptr && m->ring_idx && m->sub_cl && m->sub_cr && m->sub_nx && m->sub_ny &&
            m->sub_len && m->sub_dzl && m->sub_dzr && m->sub_ptr && m->sub_count && m->sub_lcsr && m->sub_lcsr_ptr &&
-           m->block_inst && m->block_cells;
+           m->block_inst && m->block_cells && (m->n_open == 0u || m->open_cond);
 }
+
+// The open-edge tally words must exist when the mesh has open edges.
+inline bool open_ok(const swe_mesh_t *m, const swe_state_t *s) { return m->n_open == 0u || s->open_vol; }
 
 inline bool state_ok(const swe_state_t *s) {
     return s && s->h && s->hu && s->hv && s->h_lo && s->h1 && s->hu1 && s->hv1 && s->h1_lo && s->clamp_mass &&

@@ -155,8 +155,9 @@ __global__ void __launch_bounds__(kThreads) cfl_prologue_kernel(swe_mesh_t m, sw
             const float hL = s.h[cL], huL = s.hu[cL], hvL = s.hv[cL];
             float hR, huR, hvR;
             if (cR < 0) {
-                hR = hL;
-                wall_mirror(huL, hvL, nx, ny, huR, hvR);
+                uint32_t kind = kOpenWall;
+                float value = 0.0f;
+                boundary_state(m, p, cR, hL, huL, hvL, nx, ny, hR, huR, hvR, kind, value);
             } else {
                 hR = s.h[cR];
                 huR = s.hu[cR];

@@ -58,6 +58,23 @@ __global__ void pow43_kernel(const float *x, float *out, uint32_t n) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = pow43(x[i]);
 }
 
+// The ghost state and mass flux of open edges from given cells: the device
+// half of the reference's ghost probe (tests/unit/test_gpu_open_ghost.py:45-71).
+__global__ void open_ghost_kernel(const float *cases, const uint32_t *cond, float *results, uint32_t n, Phys p) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const float *c = cases + 6ull * k;
+        const uint32_t kind = cond[2ull * k];
+        const float value = __uint_as_float(cond[2ull * k + 1]);
+        float hG, huG, hvG;
+        ghost_state(p, kind, value, c[0], c[1], c[2], c[3], c[4], hG, huG, hvG);
+        float *r = results + 4ull * k;
+        r[0] = hG;
+        r[1] = huG;
+        r[2] = hvG;
+        r[3] = boundary_mass_flux(kind, value, c[5]);
+    }
+}
+
 }  // namespace swe
 
 using namespace swe;
@@ -90,6 +107,16 @@ int swe_eft_probe(float *v, swe_stream_t stream) {
 int swe_pow43(const float *x, float *out, uint32_t n, swe_stream_t stream) {
     if (!x || !out || n == 0u) return SWE_ERR_ARGUMENT;
     pow43_kernel<<<min((n + 255u) / 256u, 4096u), 256, 0, stream>>>(x, out, n);
+    return check_launch();
+}
+
+int swe_open_ghost_probe(const float *cases, const uint32_t *cond, float *results, uint32_t n, float g,
+                         float dry_tol, swe_stream_t stream) {
+    if (!cases || !cond || !results || n == 0u) return SWE_ERR_ARGUMENT;
+    Phys p;
+    p.g = g;
+    p.dry_tol = dry_tol;
+    open_ghost_kernel<<<min((n + 255u) / 256u, 4096u), 256, 0, stream>>>(cases, cond, results, n, p);
     return check_launch();
 }
 

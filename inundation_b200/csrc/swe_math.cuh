@@ -156,6 +156,79 @@ __device__ __forceinline__ void wall_mirror(float huL, float hvL, float nx, floa
     hvR = hvL - 2.0f * (huL * nx + hvL * ny) * ny;
 }
 
+// -- open boundaries (flux.py:187-294) ----------------------------------------------------------
+// Open edge k has cR = -2 - k; its condition is the word pair (kind, value bits).
+constexpr uint32_t kOpenWall = 0u, kOpenFree = 1u, kOpenNormal = 2u, kOpenStage = 3u, kOpenInflow = 4u;
+constexpr int kOpenNewtonSteps = 4;
+
+// Cube root of x >= 0 by the Newton iteration of pow43 (no fixed-rounding pow is
+// assumed; this is one value GLSL's pow(x, 1/3) admits).
+__device__ __forceinline__ float cbrt_newton(float x) {
+    if (!(x > 0.0f)) return 0.0f;
+    float r = __uint_as_float(__float_as_uint(x) / 3u + 0x2A555555u);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) r = (2.0f * r + x / (r * r)) / 3.0f;
+    return r;
+}
+
+// Depth beyond an inflow edge of discharge q per unit width: the root of
+// -q/hG + 2 sqrt(g hG) = riemann (the outgoing characteristic), by Newton in s = sqrt(hG).
+__device__ __forceinline__ float inflow_depth(const Phys &p, float q, float riemann) {
+    const float root_g = sqrtf(p.g);
+    float s = gmax(cbrt_newton(q / (2.0f * root_g)), riemann / (2.0f * root_g));
+    for (int k = 0; k < kOpenNewtonSteps; ++k) {
+        const float f = 2.0f * root_g * s - q / (s * s) - riemann;
+        const float df = 2.0f * root_g + 2.0f * q / (s * s * s);
+        s = gmax(s - f / df, 0.5f * s);
+    }
+    return s * s;
+}
+
+// The state beyond an open edge of condition `kind` from the cell inside it.
+// value: sqrt(S)/n for NORMAL, the depth over this cell's bed for STAGE, the
+// discharge per unit width for INFLOW.
+__device__ __forceinline__ void ghost_state(const Phys &p, uint32_t kind, float value, float hL, float huL, float hvL,
+                                            float nx, float ny, float &hG, float &huG, float &hvG) {
+    const float uL = safe_vel(p, hL, huL);
+    const float vL = safe_vel(p, hL, hvL);
+    const float unL = uL * nx + vL * ny;
+    float ut = -uL * ny + vL * nx;
+    const float cL = sqrtf(p.g * gmax(hL, 0.0f));
+    float un = -unL;
+    hG = hL;
+    if (kind == kOpenFree) {
+        un = fabsf(unL);
+    } else if (kind == kOpenNormal) {
+        const float r = cbrt_newton(gmax(hL, 0.0f));
+        un = value * (r * r);
+    } else if (kind == kOpenStage) {
+        if (hL < p.dry_tol || unL < cL) {
+            hG = value;
+            un = unL + 2.0f * (cL - sqrtf(p.g * value));
+        } else {
+            un = unL;
+        }
+    } else if (kind == kOpenInflow && value > 0.0f) {
+        hG = inflow_depth(p, value, unL + 2.0f * cL);
+        un = -value / hG;
+        ut = 0.0f;
+    }
+    huG = hG * (un * nx - ut * ny);
+    hvG = hG * (un * ny + ut * nx);
+}
+
+// An inflow keeps its edge live while dry, or its volume would be lost.
+__device__ __forceinline__ bool open_forced(uint32_t kind, float value) { return kind == kOpenInflow && value > 0.0f; }
+
+// Mass flux through a boundary edge: outflow conditions never draw water in,
+// inflow carries exactly its discharge, a wall passes none.
+__device__ __forceinline__ float boundary_mass_flux(uint32_t kind, float value, float Fh) {
+    if (kind == kOpenFree || kind == kOpenNormal) return gmax(Fh, 0.0f);
+    if (kind == kOpenStage) return Fh;
+    if (kind == kOpenInflow) return -value;
+    return 0.0f;
+}
+
 // Semi-implicit momentum decay factor of a thin film (a rate, independent of the tick).
 __device__ __forceinline__ float film_drag(const Phys &p, float h, float dt) {
     const float e = kFilmDepths * p.dry_tol;

@@ -57,7 +57,7 @@ __device__ __forceinline__ void flag_pass(const swe_mesh_t &m, const swe_state_t
     }
 }
 
-template <bool COMP, bool CLAMP>
+template <bool COMP, bool CLAMP, bool OPEN>
 __global__ void __launch_bounds__(kPersistThreads, 1024 / kPersistThreads)
     persistent_steps_kernel(swe_mesh_t m, swe_state_t s, swe_sources_t src, Phys p, float cfl, int all_active,
                             uint32_t n_steps) {
@@ -93,13 +93,13 @@ __global__ void __launch_bounds__(kPersistThreads, 1024 / kPersistThreads)
         sj.items = reinterpret_cast<uint32_t *>(item_sets(cur));
         const Spread sp{lists(nxt), item_sets(nxt), epoch};
         const Spread none{};
-        if (!(ok = tiled_pass<0, COMP, CLAMP, kPersistThreads, true>(m, sj, p, cfl, smem, sh, k, computed))) break;
+        if (!(ok = tiled_pass<0, COMP, CLAMP, kPersistThreads, true, OPEN>(m, sj, p, cfl, smem, sh, k, computed))) break;
         if (step > 0u && !all_active) {
             const volatile uint32_t *sched = s.sched;
             flag_pass(m, s, lists(cur), sched[kSchedActive], lists(nxt), sched[kSchedPrevActive], epoch - 1u);
         }
         if (!(ok = grid_sync(g, flag, nothing))) break;
-        if (!(ok = tiled_pass<1, COMP, CLAMP, kPersistThreads, true>(m, sj, p, cfl, smem, sh, k, computed,
+        if (!(ok = tiled_pass<1, COMP, CLAMP, kPersistThreads, true, OPEN>(m, sj, p, cfl, smem, sh, k, computed,
                                                                       all_active ? none : sp)))
             break;
         if (src.count) {
@@ -157,10 +157,10 @@ __global__ void __launch_bounds__(kPersistThreads, 1024 / kPersistThreads)
     }
 }
 
-template <bool COMP, bool CLAMP>
+template <bool COMP, bool CLAMP, bool OPEN>
 int launch_persistent(const swe_mesh_t *m, const swe_state_t *s, const swe_params_t *p, const swe_sources_t *src,
                       uint32_t n_steps, cudaStream_t st) {
-    auto kern = persistent_steps_kernel<COMP, CLAMP>;
+    auto kern = persistent_steps_kernel<COMP, CLAMP, OPEN>;
     const size_t bytes = tiled_smem_bytes(m->max_sub_edges, m->max_sub_slots, true);
     int rc = set_smem(kern, bytes);
     if (rc) return rc;
@@ -185,14 +185,28 @@ int launch_persistent(const swe_mesh_t *m, const swe_state_t *s, const swe_param
     return SWE_OK;
 }
 
+template <bool OPEN>
+int dispatch_persistent(const swe_mesh_t *m, const swe_state_t *s, const swe_params_t *p, const swe_sources_t *src,
+                        uint32_t n_steps, cudaStream_t st) {
+    if (p->compensated)
+        return p->track_clamp ? launch_persistent<true, true, OPEN>(m, s, p, src, n_steps, st)
+                              : launch_persistent<true, false, OPEN>(m, s, p, src, n_steps, st);
+    return p->track_clamp ? launch_persistent<false, true, OPEN>(m, s, p, src, n_steps, st)
+                          : launch_persistent<false, false, OPEN>(m, s, p, src, n_steps, st);
+}
+
 int configure_persistent(const swe_mesh_t *mesh, int *blocks_per_sm) {
     const size_t bytes = tiled_smem_bytes(mesh->max_sub_edges, mesh->max_sub_slots, true);
-    int rc = set_smem(persistent_steps_kernel<true, false>, bytes);
-    if (!rc) rc = set_smem(persistent_steps_kernel<true, true>, bytes);
-    if (!rc) rc = set_smem(persistent_steps_kernel<false, false>, bytes);
-    if (!rc) rc = set_smem(persistent_steps_kernel<false, true>, bytes);
+    int rc = set_smem(persistent_steps_kernel<true, false, false>, bytes);
+    if (!rc) rc = set_smem(persistent_steps_kernel<true, true, false>, bytes);
+    if (!rc) rc = set_smem(persistent_steps_kernel<false, false, false>, bytes);
+    if (!rc) rc = set_smem(persistent_steps_kernel<false, true, false>, bytes);
+    if (!rc) rc = set_smem(persistent_steps_kernel<true, false, true>, bytes);
+    if (!rc) rc = set_smem(persistent_steps_kernel<true, true, true>, bytes);
+    if (!rc) rc = set_smem(persistent_steps_kernel<false, false, true>, bytes);
+    if (!rc) rc = set_smem(persistent_steps_kernel<false, true, true>, bytes);
     if (rc) return rc;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, persistent_steps_kernel<true, false>,
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, persistent_steps_kernel<true, false, false>,
                                                          kPersistThreads, bytes) == cudaSuccess
                ? SWE_OK
                : SWE_ERR_CUDA;
@@ -204,7 +218,8 @@ using namespace swe;
 
 extern "C" int swe_steps(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params_t *params,
                          const swe_sources_t *sources, uint32_t n_steps, swe_stream_t stream) {
-    if (!mesh_ok(mesh) || !state_ok(state) || !params || !sources || params->kernel > 2u) return SWE_ERR_ARGUMENT;
+    if (!mesh_ok(mesh) || !state_ok(state) || !open_ok(mesh, state) || !params || !sources || params->kernel > 2u)
+        return SWE_ERR_ARGUMENT;
     if (n_steps == 0u) return SWE_OK;
     if (params->kernel < 2u) {
         for (uint32_t k = 0; k < n_steps; ++k) {
@@ -216,9 +231,6 @@ extern "C" int swe_steps(const swe_mesh_t *mesh, const swe_state_t *state, const
     if (!state->sync || !state->marks) return SWE_ERR_ARGUMENT;
     if (mesh->max_sub_edges > 2047u || mesh->max_sub_slots > 2047u || mesh->n_inst > 1023u) return SWE_ERR_TOO_LARGE;
     if (sources->count && (!sources->cells || !sources->rate)) return SWE_ERR_ARGUMENT;
-    if (params->compensated)
-        return params->track_clamp ? launch_persistent<true, true>(mesh, state, params, sources, n_steps, stream)
-                                   : launch_persistent<true, false>(mesh, state, params, sources, n_steps, stream);
-    return params->track_clamp ? launch_persistent<false, true>(mesh, state, params, sources, n_steps, stream)
-                               : launch_persistent<false, false>(mesh, state, params, sources, n_steps, stream);
+    return mesh->n_open ? dispatch_persistent<true>(mesh, state, params, sources, n_steps, stream)
+                        : dispatch_persistent<false>(mesh, state, params, sources, n_steps, stream);
 }

@@ -48,9 +48,9 @@ inline size_t block_smem_bytes(uint32_t max_tile_edges) {
 // 256-cell blocks, plain loads: persistent CTAs stride over the active list.
 // sums != nullptr: also store every computed cell's gathered sums (sdh, sdhu,
 // sdhv at sums[i], sums[n + i], sums[2n + i], n = padded cells), the record
-// the adjoint reverses.
+// the adjoint reverses. OPEN: the mesh has open edges.
 // ---------------------------------------------------------------------------
-template <int STAGE, bool COMP, bool CLAMP>
+template <int STAGE, bool COMP, bool CLAMP, bool OPEN>
 __global__ void __launch_bounds__(kThreads)
     stage_block_kernel(swe_mesh_t m, swe_state_t s, Phys p, float cfl, float *sums) {
     const uint32_t cap = (m.max_tile_edges + 3u) & ~3u;
@@ -73,19 +73,26 @@ __global__ void __launch_bounds__(kThreads)
             const float nx = m.tile_nx[e], ny = m.tile_ny[e];
             float hL, huL, hvL, hR, huR, hvR;
             load_state<STAGE>(s, cL, hL, huL, hvL);
+            uint32_t kind = kOpenWall;
+            float value = 0.0f;
             if (cR < 0) {
-                hR = hL;
-                wall_mirror(huL, hvL, nx, ny, huR, hvR);
+                if (OPEN) {
+                    boundary_state(m, p, cR, hL, huL, hvL, nx, ny, hR, huR, hvR, kind, value);
+                } else {
+                    hR = hL;
+                    wall_mirror(huL, hvL, nx, ny, huR, hvR);
+                }
             } else {
                 load_state<STAGE>(s, cR, hR, huR, hvR);
             }
-            const bool live = !(hL < p.dry_tol && hR < p.dry_tol);
+            const bool live = !(hL < p.dry_tol && hR < p.dry_tol) || (OPEN && open_forced(kind, value));
             t.live[j] = live;
             if (!live) continue;
             float c;
-            edge_words(p, cR, nx, ny, m.tile_len[e], m.tile_dzl[e], m.tile_dzr[e], hL, huL, hvL, hR, huR, hvR,
-                       t.F0[j], t.L1[j], t.L2[j], t.R1[j], t.R2[j], c);
+            edge_words<OPEN>(p, cR, nx, ny, m.tile_len[e], m.tile_dzl[e], m.tile_dzr[e], hL, huL, hvL, hR, huR, hvR,
+                       t.F0[j], t.L1[j], t.L2[j], t.R1[j], t.R2[j], c, kind, value);
             if (STAGE == 1) t.C[j] = c;
+            if (OPEN && cR < -1) tally_open(s.open_vol, static_cast<uint32_t>(-2 - cR), (0.5f * dt) * t.F0[j]);
         }
         __syncthreads();
 
@@ -139,7 +146,7 @@ __global__ void __launch_bounds__(kThreads)
         atomicAdd(reinterpret_cast<unsigned long long *>(s.sched + kSchedComputed), computed);
 }
 
-template <int STAGE, bool COMP, bool CLAMP>
+template <int STAGE, bool COMP, bool CLAMP, bool OPEN>
 __global__ void __launch_bounds__(kTileThreads, 8)
     stage_tiled_kernel(swe_mesh_t m, swe_state_t s, Phys p, float cfl, float *sums) {
     if (blockIdx.x >= s.sched[kSchedItems]) return;
@@ -153,7 +160,8 @@ __global__ void __launch_bounds__(kTileThreads, 8)
     __syncthreads();
     uint32_t k = 0;
     uint64_t computed = 0;
-    if (!tiled_pass<STAGE, COMP, CLAMP, kTileThreads>(m, s, p, cfl, smem, sh, k, computed, Spread{}, sums)) return;
+    if (!tiled_pass<STAGE, COMP, CLAMP, kTileThreads, false, OPEN>(m, s, p, cfl, smem, sh, k, computed, Spread{}, sums))
+        return;
     if (STAGE == 1 && threadIdx.x == 0 && computed)
         atomicAdd(reinterpret_cast<unsigned long long *>(s.sched + kSchedComputed), computed);
 }
@@ -161,12 +169,12 @@ __global__ void __launch_bounds__(kTileThreads, 8)
 // ---------------------------------------------------------------------------
 // Host side.
 // ---------------------------------------------------------------------------
-template <int STAGE, bool COMP, bool CLAMP>
+template <int STAGE, bool COMP, bool CLAMP, bool OPEN>
 int launch_stage(const swe_mesh_t *m, const swe_state_t *s, const swe_params_t *p, cudaStream_t st,
                  float *sums = nullptr) {
     const Phys ph{p->g, p->dry_tol};
     if (p->kernel == 1u) {
-        auto kern = stage_block_kernel<STAGE, COMP, CLAMP>;
+        auto kern = stage_block_kernel<STAGE, COMP, CLAMP, OPEN>;
         const size_t bytes = block_smem_bytes(m->max_tile_edges);
         int rc = set_smem(kern, bytes);
         if (rc) return rc;
@@ -174,7 +182,7 @@ int launch_stage(const swe_mesh_t *m, const swe_state_t *s, const swe_params_t *
         kern<<<grid, kThreads, bytes, st>>>(*m, *s, ph, p->cfl, sums);
         return check_launch();
     }
-    auto kern = stage_tiled_kernel<STAGE, COMP, CLAMP>;
+    auto kern = stage_tiled_kernel<STAGE, COMP, CLAMP, OPEN>;
     const size_t bytes = tile_plan(m->max_sub_edges, m->max_sub_slots, STAGE ? 10u : 6u).total;
     int rc = set_smem(kern, bytes);
     if (rc) return rc;
@@ -182,22 +190,31 @@ int launch_stage(const swe_mesh_t *m, const swe_state_t *s, const swe_params_t *
     return check_launch();
 }
 
+template <int STAGE, bool OPEN>
+int dispatch_open(const swe_mesh_t *m, const swe_state_t *s, const swe_params_t *p, cudaStream_t st, float *sums) {
+    if (p->compensated) {
+        return p->track_clamp ? launch_stage<STAGE, true, true, OPEN>(m, s, p, st, sums)
+                              : launch_stage<STAGE, true, false, OPEN>(m, s, p, st, sums);
+    }
+    return p->track_clamp ? launch_stage<STAGE, false, true, OPEN>(m, s, p, st, sums)
+                          : launch_stage<STAGE, false, false, OPEN>(m, s, p, st, sums);
+}
+
 template <int STAGE>
 int dispatch_stage(const swe_mesh_t *m, const swe_state_t *s, const swe_params_t *p, cudaStream_t st,
                    float *sums = nullptr) {
-    if (p->compensated) {
-        return p->track_clamp ? launch_stage<STAGE, true, true>(m, s, p, st, sums)
-                              : launch_stage<STAGE, true, false>(m, s, p, st, sums);
-    }
-    return p->track_clamp ? launch_stage<STAGE, false, true>(m, s, p, st, sums)
-                          : launch_stage<STAGE, false, false>(m, s, p, st, sums);
+    return m->n_open ? dispatch_open<STAGE, true>(m, s, p, st, sums) : dispatch_open<STAGE, false>(m, s, p, st, sums);
 }
 
 template <int STAGE, bool COMP, bool CLAMP>
 int configure_stage(const swe_mesh_t *m) {
-    int rc = set_smem(stage_block_kernel<STAGE, COMP, CLAMP>, block_smem_bytes(m->max_tile_edges));
-    if (rc) return rc;
-    return set_smem(stage_tiled_kernel<STAGE, COMP, CLAMP>, tile_plan(m->max_sub_edges, m->max_sub_slots, STAGE ? 10u : 6u).total);
+    const size_t block = block_smem_bytes(m->max_tile_edges);
+    const size_t tiled = tile_plan(m->max_sub_edges, m->max_sub_slots, STAGE ? 10u : 6u).total;
+    int rc = set_smem(stage_block_kernel<STAGE, COMP, CLAMP, false>, block);
+    if (!rc) rc = set_smem(stage_block_kernel<STAGE, COMP, CLAMP, true>, block);
+    if (!rc) rc = set_smem(stage_tiled_kernel<STAGE, COMP, CLAMP, false>, tiled);
+    if (!rc) rc = set_smem(stage_tiled_kernel<STAGE, COMP, CLAMP, true>, tiled);
+    return rc;
 }
 
 int configure_persistent(const swe_mesh_t *mesh, int *blocks_per_sm);  // swe_persist.cu
@@ -224,17 +241,18 @@ int swe_configure(const swe_mesh_t *mesh, int kernel, int *blocks_per_sm) {
     cudaError_t err;
     if (kernel == 0) {
         err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            blocks_per_sm, stage_tiled_kernel<1, true, false>, kTileThreads,
+            blocks_per_sm, stage_tiled_kernel<1, true, false, false>, kTileThreads,
             tile_plan(mesh->max_sub_edges, mesh->max_sub_slots, 10u).total);
     } else {
-        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, stage_block_kernel<1, true, false>, kThreads,
+        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, stage_block_kernel<1, true, false, false>, kThreads,
                                                             block_smem_bytes(mesh->max_tile_edges));
     }
     return err == cudaSuccess ? SWE_OK : SWE_ERR_CUDA;
 }
 
 int swe_stage(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params_t *params, int stage, swe_stream_t stream) {
-    if (!mesh_ok(mesh) || !state_ok(state) || !params || params->kernel > 1u) return SWE_ERR_ARGUMENT;
+    if (!mesh_ok(mesh) || !state_ok(state) || !open_ok(mesh, state) || !params || params->kernel > 1u)
+        return SWE_ERR_ARGUMENT;
     if (stage == 0) return dispatch_stage<0>(mesh, state, params, stream);
     if (stage == 1) return dispatch_stage<1>(mesh, state, params, stream);
     return SWE_ERR_ARGUMENT;
@@ -242,7 +260,7 @@ int swe_stage(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params
 
 int swe_stage_taped(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params_t *params, int stage,
                     float *sums, swe_stream_t stream) {
-    if (!mesh_ok(mesh) || !state_ok(state) || !params || !sums) return SWE_ERR_ARGUMENT;
+    if (!mesh_ok(mesh) || !state_ok(state) || !params || !sums || mesh->n_open) return SWE_ERR_ARGUMENT;
     if (stage == 0) return dispatch_stage<0>(mesh, state, params, stream, sums);
     if (stage == 1) return dispatch_stage<1>(mesh, state, params, stream, sums);
     return SWE_ERR_ARGUMENT;

@@ -85,15 +85,30 @@ __device__ __forceinline__ void update_cell(const swe_state_t &s, const Phys &p,
 }
 
 // Flux of one edge from its two cell states: the five gather words and the
-// corrector's CFL word (resident.py:254-284).
+// corrector's CFL word (resident.py:254-284). On an open edge (cR < -1,
+// condition kind/value) the mass flux follows the condition, and an
+// outflow-only edge whose flux would draw water in is redone as a wall, its
+// momentum included (flux.py:284-294). OPEN: the mesh may have open edges.
+template <bool OPEN>
 __device__ __forceinline__ void edge_words(const Phys &p, int cR, float nx, float ny, float len, float dzL,
                                            float dzR, float hL, float huL, float hvL, float hR, float huR,
                                            float hvR, float &w0, float &w1, float &w2, float &w3, float &w4,
-                                           float &w5) {
+                                           float &w5, uint32_t kind = kOpenWall, float value = 0.0f) {
     float hLs, hqnL, hqtL, hRs, hqnR, hqtR, Fh, Fhn, Fht, smax;
     face_states(p, hL, huL, hvL, dzL, hR, huR, hvR, dzR, nx, ny, hLs, hqnL, hqtL, hRs, hqnR, hqtR);
     hllc(p, hLs, hqnL, hqtL, hRs, hqnR, hqtR, Fh, Fhn, Fht, smax);
-    if (cR < 0) Fh = 0.0f;  // a wall passes no mass
+    if (OPEN && cR < -1) {
+        if ((kind == kOpenFree || kind == kOpenNormal) && Fh < 0.0f) {
+            ghost_state(p, kOpenWall, 0.0f, hL, huL, hvL, nx, ny, hR, huR, hvR);
+            face_states(p, hL, huL, hvL, dzL, hR, huR, hvR, dzR, nx, ny, hLs, hqnL, hqtL, hRs, hqnR, hqtR);
+            hllc(p, hLs, hqnL, hqtL, hRs, hqnR, hqtR, Fh, Fhn, Fht, smax);
+            Fh = 0.0f;
+        } else {
+            Fh = boundary_mass_flux(kind, value, Fh);
+        }
+    } else if (cR < 0) {
+        Fh = 0.0f;  // a wall passes no mass
+    }
     const float Fhu = Fhn * nx - Fht * ny;
     const float Fhv = Fhn * ny + Fht * nx;
     const float SL_g = 0.5f * p.g * (hL * hL - hLs * hLs);
@@ -284,7 +299,8 @@ __host__ __device__ inline size_t tiled_smem_bytes(uint32_t max_edges, uint32_t 
 // columns in_col..in_col+3 of B.c (h, hu, hv, h_lo), the committed state of the
 // corrector in com_col..com_col+3. F == nullptr: the flux words overwrite the
 // consumed records; otherwise they go to F (7 x capE words) and the records stay.
-template <int STAGE, bool COMP, bool CLAMP, int TPB>
+// OPEN: the mesh has open edges (right cell -2 - k), with ghosts and tallies.
+template <int STAGE, bool COMP, bool CLAMP, int TPB, bool OPEN>
 __device__ __forceinline__ void tile_compute(const swe_mesh_t &m, const swe_state_t &s, const Phys &p, float cfl,
                                              const TileBuf &B, const Item &it, float dt, uint32_t in_col,
                                              uint32_t com_col, float *F, uint32_t capE, uint32_t *red,
@@ -313,9 +329,15 @@ __device__ __forceinline__ void tile_compute(const swe_mesh_t &m, const swe_stat
         } else {
             load_state<STAGE>(s, cL, hL, huL, hvL);
         }
+        uint32_t kind = kOpenWall;
+        float value = 0.0f;
         if (cR < 0) {
-            hR = hL;
-            wall_mirror(huL, hvL, nx, ny, huR, hvR);
+            if (OPEN) {
+                boundary_state(m, p, cR, hL, huL, hvL, nx, ny, hR, huR, hvR, kind, value);
+            } else {
+                hR = hL;
+                wall_mirror(huL, hvL, nx, ny, huR, hvR);
+            }
         } else {
             const uint32_t lR = static_cast<uint32_t>(cR - base);
             if (lR < static_cast<uint32_t>(kTileCells)) {
@@ -326,12 +348,14 @@ __device__ __forceinline__ void tile_compute(const swe_mesh_t &m, const swe_stat
                 load_state<STAGE>(s, cR, hR, huR, hvR);
             }
         }
-        const bool live = !(hL < p.dry_tol && hR < p.dry_tol);
+        const bool live = !(hL < p.dry_tol && hR < p.dry_tol) || (OPEN && open_forced(kind, value));
         const float len = B.len[j], dzl = B.dzl[j], dzr = B.dzr[j];
         live_w[j] = live ? 1 : 0;
         if (!live) continue;
         float w0, w1, w2, w3, w4, w5;
-        edge_words(p, cR, nx, ny, len, dzl, dzr, hL, huL, hvL, hR, huR, hvR, w0, w1, w2, w3, w4, w5);
+        edge_words<OPEN>(p, cR, nx, ny, len, dzl, dzr, hL, huL, hvL, hR, huR, hvR, w0, w1, w2, w3, w4, w5, kind,
+                         value);
+        if (OPEN && cR < -1) tally_open(s.open_vol, static_cast<uint32_t>(-2 - cR), (0.5f * dt) * w0);
         W0[j] = w0;
         W1[j] = w1;
         W2[j] = w2;
@@ -399,7 +423,7 @@ __device__ __forceinline__ void tile_compute(const swe_mesh_t &m, const swe_stat
 // predictor's staged tile without staging anything.
 // Returns false when staged data did not arrive within the wait bound (the
 // copies in flight have had one more bounded wait; the caller must stop).
-template <int STAGE, bool COMP, bool CLAMP, int TPB, bool KEEP = false>
+template <int STAGE, bool COMP, bool CLAMP, int TPB, bool KEEP, bool OPEN>
 __device__ bool tiled_pass(const swe_mesh_t &m, const swe_state_t &s, const Phys &p, float cfl, unsigned char *smem,
                            TiledShared<TPB> &sh, uint32_t &k, uint64_t &computed, const Spread &sp = Spread{},
                            float *sums = nullptr) {
@@ -418,7 +442,7 @@ __device__ bool tiled_pass(const swe_mesh_t &m, const swe_state_t &s, const Phys
         const uint32_t kb = (k - 1u) & 1u;
         const uint32_t dt_bits = dts[kb];
         if (dt_bits != 0u)
-            tile_compute<1, COMP, CLAMP, TPB>(m, s, p, cfl, tile_buf(smem, L, kb), unpack(items[kb]),
+            tile_compute<1, COMP, CLAMP, TPB, OPEN>(m, s, p, cfl, tile_buf(smem, L, kb), unpack(items[kb]),
                                               __uint_as_float(dt_bits), 6u, 0u, F, L.capE, red, computed, false, sp, sums);
         __syncthreads();
         return true;
@@ -476,7 +500,7 @@ __device__ bool tiled_pass(const swe_mesh_t &m, const swe_state_t &s, const Phys
         }
         const uint32_t dt_bits = dts[k & 1u];
         if (dt_bits != 0u)
-            tile_compute<STAGE, COMP, CLAMP, TPB>(m, s, p, cfl, B, unpack(items[k & 1u]), __uint_as_float(dt_bits), 0u,
+            tile_compute<STAGE, COMP, CLAMP, TPB, OPEN>(m, s, p, cfl, B, unpack(items[k & 1u]), __uint_as_float(dt_bits), 0u,
                                                   6u, F, L.capE, red, computed, keep_pred, sp, sums);
         // This buffer is refilled by bulk copies two items on.
         fence_proxy_async();

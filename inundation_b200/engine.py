@@ -24,7 +24,7 @@ from numpy.typing import NDArray
 from . import native
 from .layout import TileLayout
 from .sources import NO_HYDROGRAPH, Hydrograph
-from .tuning import B200_BACKEND, CFL_DEFAULT, DRY_TOL_DEFAULT, GRAVITY_G
+from .tuning import ACTIVE_BLOCK_CELLS, B200_BACKEND, CFL_DEFAULT, DRY_TOL_DEFAULT, GRAVITY_G, OPEN_INFLOW, OPEN_STAGE
 
 # Host mirror of swe_ctrl_t (the reference's RESIDENT_CTRL_DTYPE, 48 bytes;
 # the reference's padding word carries the device error flag).
@@ -117,6 +117,9 @@ class ResidentEngine:
         t["lcsr"] = self._dev(B.lcsr.view(np.int16))
         t["sub_lcsr"] = self._dev(S.lcsr_blk.view(np.int16))
         t["sub_lcsr_ptr"] = self._dev(_i32(S.lcsr_ptr))
+        self.n_open = L.n_open
+        if L.n_open:  # conditions start as walls; the pointer stays fixed, so graphs see every update
+            t["open_cond"] = torch.zeros(2 * L.n_open, dtype=torch.int32, device=self.device)
         self._mesh_t = t
         m = native.SweMesh()
         m.n_cells = L.n_padded_cells
@@ -127,6 +130,7 @@ class ResidentEngine:
         m.max_sub_slots = S.max_slots
         for name, tensor in t.items():
             setattr(m, name, tensor.data_ptr())
+        m.n_open = L.n_open
         self._mesh = m
         self._sms = torch.cuda.get_device_properties(self.device).multi_processor_count
         self._per_sm: dict[int, int] = {}
@@ -170,6 +174,7 @@ class ResidentEngine:
         self._dt_buf = self._dev(dt.view(np.int32))
         self._ctrl_dev = torch.zeros(6 * ni, dtype=torch.int64, device=dev)
         self._sync = torch.zeros(64, dtype=torch.int32, device=dev)  # grid barrier words of the persistent kernel
+        self._open_vol = torch.zeros(4 * max(self.n_open, 1), dtype=torch.float32, device=dev)  # out, in pairs
         self._ctrl_pinned = torch.zeros(6 * ni, dtype=torch.int64).pin_memory()
         self._ctrl = self._ctrl_pinned.numpy().view(RESIDENT_CTRL_DTYPE)
         self._sched_pinned = torch.zeros(8, dtype=torch.int64).pin_memory()
@@ -187,6 +192,7 @@ class ResidentEngine:
         s.ctrl = self._ctrl_dev.data_ptr()
         s.sync = self._sync.data_ptr()
         s.marks = self._marks.data_ptr()
+        s.open_vol = self._open_vol.data_ptr() if self.n_open else None
         self._state = s
 
     def _params(self) -> native.SweParams:
@@ -301,6 +307,45 @@ class ResidentEngine:
         with torch.cuda.stream(self._stream):
             self._t[name][self._inst_range(inst)].copy_(src)
         self._stream.synchronize()
+
+    # -- open boundaries ----------------------------------------------------------------
+    def set_open_edge_conditions(self, kinds: NDArray[np.uint32], values: NDArray[np.float32]) -> None:
+        """Every open edge's condition, by open index, and the blocks it forces.
+
+        A block with an open edge that can bring water in (an inflow or a stage
+        with a positive value) is forced: it and its two-ring stay active while
+        the condition holds (``inundation/vulkan/gpu_resident_batch.py:447-458``).
+        Takes effect at the next start of a run (its prologue rebuilds the lists).
+        """
+        kinds = np.asarray(kinds, np.uint32).ravel()
+        values = np.asarray(values, np.float32).ravel()
+        if kinds.size != self.n_open or values.size != self.n_open:
+            raise ValueError(f"expected {self.n_open} open edges, got {kinds.size} kinds and {values.size} values")
+        if not self.n_open:
+            return
+        words = np.empty(2 * self.n_open, np.uint32)
+        words[0::2] = kinds
+        words[1::2] = values.view(np.uint32)
+        forced = np.zeros(self.n_blocks, np.int32)
+        brings_water = np.isin(kinds, (OPEN_INFLOW, OPEN_STAGE)) & (values > 0.0)
+        forced[self.layout.open_cells[brings_water] // ACTIVE_BLOCK_CELLS] = 1
+        with torch.cuda.stream(self._stream):
+            self._mesh_t["open_cond"].copy_(torch.from_numpy(words.view(np.int32)))
+            self._blk.view(self.n_blocks, 3)[:, 2].copy_(torch.from_numpy(forced))
+        self._stream.synchronize()
+
+    def download_open_edge_volumes(self) -> NDArray[np.float64]:
+        """``(n_open, 2)`` volume out of and into the mesh through every open edge, float64."""
+        if not self.n_open:
+            return np.zeros((0, 2), np.float64)
+        with torch.cuda.stream(self._stream):
+            words = self._open_vol.cpu().numpy().astype(np.float64)
+        pairs = words[: 4 * self.n_open].reshape(-1, 4)
+        return np.column_stack([pairs[:, 0] + pairs[:, 1], pairs[:, 2] + pairs[:, 3]])
+
+    def reset_open_volumes(self) -> None:
+        with torch.cuda.stream(self._stream):
+            self._open_vol.zero_()
 
     def download_block_flags(self) -> NDArray[np.uint32]:
         """``(n_blocks, 3)`` flags: wet, active, forced."""

@@ -20,6 +20,10 @@ the same terms in the same order as the reference.
 Two tile sizes are built: 256 cells (one active-set block; the kernels of
 the prologue, the sources and the plain stage kernel) and 64 cells (four
 compute tiles per block; the tiled stage kernel).
+
+Open boundary edges keep the reference's numbering (``inundation/vulkan/solver.py:236-243``):
+an edge whose right cell is ``-2 - k`` is open edge ``k``. Like a wall it sits
+in the tile of its left cell only.
 """
 
 from __future__ import annotations
@@ -77,6 +81,11 @@ class TileLayout:
     block_cells: NDArray[np.uint32]  # real cells of every block
     inst_cell_offset: NDArray[np.int64]  # first cell of every instance (a multiple of 256)
     inst_cells: NDArray[np.int64]  # real cells of every instance
+    open_cells: NDArray[np.int64] | None = None  # left (padded) cell of every open edge, by open index
+
+    @property
+    def n_open(self) -> int:
+        return 0 if self.open_cells is None else int(self.open_cells.size)
 
     @property
     def n_inst(self) -> int:
@@ -189,8 +198,12 @@ def _build(geom) -> TileLayout:
     n, n_e = int(geom.N), int(geom.E)
     if n == 0 or n_e == 0:
         raise ValueError("mesh has no cells or no edges")
-    if (geom.edge_cellR < -1).any():
-        raise ValueError("open boundary edges are not supported by this layout")
+    open_mask = np.asarray(geom.edge_cellR) < -1
+    open_k = (-2 - np.asarray(geom.edge_cellR)[open_mask]).astype(np.int64)
+    if open_k.size and not np.array_equal(np.sort(open_k), np.arange(open_k.size)):
+        raise ValueError("open edges must be numbered -2 - k for k = 0 .. n_open - 1, each once")
+    open_cells = np.empty(open_k.size, dtype=np.int64)
+    open_cells[open_k] = np.asarray(geom.edge_cellL)[open_mask]
     bc = ACTIVE_BLOCK_CELLS
     n_blk = num_blocks(n, bc)
     order = edge_order_by_block(geom.edge_cellL, bc)
@@ -216,6 +229,7 @@ def _build(geom) -> TileLayout:
         block_cells=np.full(n_blk, bc, np.uint32),
         inst_cell_offset=np.zeros(1, np.int64),
         inst_cells=np.array([n], np.int64),
+        open_cells=open_cells,
     )
 
 
@@ -258,6 +272,7 @@ def build_batch_layout(geoms: list[MeshGeometry]) -> TileLayout:
     ptr = np.zeros(total + 1, dtype=np.int64)
     area = np.ones(total, dtype=np.float32)
     signed, cl, cr = [], [], []
+    open_base = 0  # open edges keep their order, numbered on from the previous instances'
     for i, g in enumerate(geoms):
         o, n = int(offs[i]), int(g.N)
         gptr = g.cell_edge_ptr.astype(np.int64)
@@ -267,7 +282,8 @@ def build_batch_layout(geoms: list[MeshGeometry]) -> TileLayout:
         signed.append(g.cell_edge_idx_signed.astype(np.int64) + 2 * int(e_offs[i]))
         cl.append(g.edge_cellL.astype(np.int64) + o)
         r = g.edge_cellR.astype(np.int64)
-        cr.append(np.where(r >= 0, r + o, r))
+        cr.append(np.where(r >= 0, r + o, np.where(r < -1, r - open_base, r)))
+        open_base += int((r < -1).sum())
     cat = lambda name: np.concatenate([getattr(g, name) for g in geoms]).astype(np.float32)  # noqa: E731
     geom = _Concatenated(
         N=total,

@@ -6,6 +6,7 @@
 * ``fractal_dem``: spectral synthesis of a 1/f^beta surface (random phases,
   amplitude k^(-beta/2)), scaled to a relief and sampled at the centroids.
 * ``gaussian_bumps``, ``carve_channel``: analytic bed features.
+* ``channel_grid``: a straight rectangular channel (the open-boundary cases).
 
 All generators take a seed and are deterministic for it.
 """
@@ -67,6 +68,21 @@ def quad_grid(nx: int, ny: int, dx: float) -> PolygonMesh:
     base = (j * (nx + 1) + i).ravel()
     faces = np.column_stack([base, base + 1, base + nx + 2, base + nx + 1]).astype(np.int32)
     return PolygonMesh(verts=verts, faces=faces.ravel(), offsets=np.arange(0, 4 * nx * ny + 1, 4, dtype=np.int32))
+
+
+def channel_grid(cells: int, across: int, length: float, width: float) -> PolygonMesh:
+    """A straight channel of ``cells`` by ``across`` rectangles on [0, length] x [0, width].
+
+    Cell k (original order) is column k % cells, row k // cells, so centres
+    along the channel repeat every ``cells`` cells.
+    """
+    xs, ys = np.meshgrid(np.linspace(0.0, length, cells + 1), np.linspace(0.0, width, across + 1))
+    verts = np.column_stack([xs.ravel(), ys.ravel()]).astype(np.float64)
+    j, i = np.meshgrid(np.arange(across), np.arange(cells), indexing="ij")
+    base = (j * (cells + 1) + i).ravel()
+    faces = np.column_stack([base, base + 1, base + cells + 2, base + cells + 1]).astype(np.int32)
+    return PolygonMesh(verts=verts, faces=faces.ravel(),
+                       offsets=np.arange(0, 4 * cells * across + 1, 4, dtype=np.int32))
 
 
 def fractal_dem(

@@ -40,6 +40,7 @@ _SIGNATURES: dict[str, tuple[list, object]] = {
     "swe_volume_fp64_noalloc": ([_P, _P, _P, _U32, _P, _P], ctypes.c_int),
     "swe_eft_probe": ([_P, _P], ctypes.c_int),
     "swe_pow43": ([_P, _P, _U32, _P], ctypes.c_int),
+    "swe_open_ghost_probe": ([_P, _P, _P, _U32, ctypes.c_float, ctypes.c_float, _P], ctypes.c_int),
     "swe_status_string": ([ctypes.c_int], ctypes.c_char_p),
     "swe_bed_steps": ([_P, _P, _P, _P, _U32, _P, _P, _U32, _P], ctypes.c_int),
     "swe_stage_taped": ([_P, _P, _P, ctypes.c_int, _P, _P], ctypes.c_int),
@@ -65,6 +66,8 @@ class SweMesh(ctypes.Structure):
             "sub_cl", "sub_cr", "sub_nx", "sub_ny", "sub_len", "sub_dzl", "sub_dzr", "sub_ptr", "sub_count",
             "sub_lcsr", "sub_lcsr_ptr",
         )],
+        ("n_open", _U32),
+        ("open_cond", _P),
     ]
 
 
@@ -73,7 +76,7 @@ class SweState(ctypes.Structure):
         (name, _P)
         for name in (
             "h", "hu", "hv", "h_lo", "h1", "hu1", "hv1", "h1_lo", "clamp_mass", "blk", "active_list", "items",
-            "sched", "dt_buf", "ctrl", "sync", "marks",
+            "sched", "dt_buf", "ctrl", "sync", "marks", "open_vol",
         )
     ]
 

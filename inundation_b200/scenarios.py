@@ -16,6 +16,9 @@ name.
   200 gauges, a seeded "true" Manning field.
 * ``batch_member``  -- one of the batched scenarios: N cells, own DEM, n in
   [0.02, 0.06], triangular inflow of 10-300 m^3/s peaking at 20 min, initially dry.
+* ``open_channel``  -- a straight sloped channel of rectangles whose two ends are
+  open stretches (``meta["open_edges"]``: upstream, downstream), the layout of
+  the reference's open-boundary cases (``inundation/bench/open_boundary.py``).
 """
 
 from __future__ import annotations
@@ -26,7 +29,8 @@ import numpy as np
 from numpy.typing import NDArray
 
 from .mesh.geometry import MeshGeometry, build_geometry, hilbert_reorder, with_bed
-from .mesh.synthetic import carve_channel, fractal_dem, gaussian_bumps, voronoi_mesh
+from .mesh.boundaries import select_boundary_edges
+from .mesh.synthetic import carve_channel, channel_grid, fractal_dem, gaussian_bumps, voronoi_mesh
 from .sources import Hydrograph, triangular_knots
 from .tuning import DRY_TOL_DEFAULT
 
@@ -173,3 +177,24 @@ def calibration(n_cells: int = 250_000, seed: int = 5, knots: int = 32, gauges: 
 def batch_sizes(count: int = 64, lo: int = 20_000, hi: int = 500_000, seed: int = 4) -> list[int]:
     rng = np.random.default_rng(seed)
     return [int(v) for v in np.exp(rng.uniform(np.log(lo), np.log(hi), count)).round()]
+
+
+def open_channel(cells: int = 300, across: int = 20, length: float = 3000.0, width: float = 200.0,
+                 slope: float = 1e-3, manning: float = 0.03, depth: float = 0.0, bed_top: float = 10.0) -> Scenario:
+    """A channel falling ``slope`` in +x from ``bed_top``, ``depth`` of still water, open at both ends.
+
+    ``meta["open_edges"]`` holds the wall edges at x = 0 and at x = length (the
+    reference's ``Channel.end`` stretches, tolerance a quarter cell).
+    """
+    mesh = channel_grid(cells, across, length, width)
+    dx = length / cells
+    x = np.tile((np.arange(cells) + 0.5) * dx, across)
+    zb = (bed_top - slope * x).astype(np.float32)
+    geom = build_geometry(mesh.verts, mesh.faces, mesh.offsets, zb_from_file=zb)
+    geom = hilbert_reorder(geom, verbose=False)[0]
+    ends = [select_boundary_edges(geom, [(xe, 0.0), (xe, width)], 0.25 * dx) for xe in (0.0, length)]
+    h0 = np.full(geom.N, depth, np.float32)
+    z = np.zeros(geom.N, np.float32)
+    return Scenario("open_channel", geom, h0, z, z.copy(), np.full(geom.N, manning, np.float32), t_end=60.0,
+                    dt_max=1.0, dt_init=0.01,
+                    meta={"open_edges": ends, "slope": slope, "manning": manning, "dx": dx, "width": width})

@@ -18,6 +18,11 @@
  *   block_mark, block_dilate       resident.py:738-802
  *   cfl_edge_gather, cfl_gather    resident.py:528-607
  *   step_control                   resident.py:813-882
+ *   open_ghost, inflow_depth, boundary_mass_flux, outflow-only redo
+ *                                  flux.py:187-294, resident.py:127-145
+ *   tally_resident                 resident.py:617-660, one pair per open
+ *                                  edge as the reference's base solver keeps
+ *                                  them (inundation/vulkan/solver.py:432-440)
  *
  * Every expression keeps the GLSL evaluation order; it is compiled with
  * -ffp-contract=off so no multiply-add is fused. GLSL min/max/clamp are
@@ -81,6 +86,11 @@ typedef struct {
     const uint32_t *knot_ptr;
     const float *knot_t;
     const float *knot_q;
+    /* Open edges: right cell -2 - k is open edge k, with condition words
+       open_cond[2k] (kind) and open_cond[2k + 1] (value bits); open_vol holds
+       4 words per open edge (out hi, lo, in hi, lo). NULL without open edges. */
+    const uint32_t *open_cond;
+    float *open_vol;
 } oracle_t;
 
 static inline uint32_t fbits(float f) { uint32_t u; memcpy(&u, &f, 4); return u; }
@@ -201,6 +211,95 @@ static void add_compensated(float hi, float loi, float inc, float *h_new, float 
     if (*h_new < 0.0f || (*h_new == 0.0f && *lo_new < 0.0f)) { *h_new = 0.0f; *lo_new = 0.0f; }
 }
 
+/* ---- open boundaries (flux.py:187-294) ---------------------------------------------------------- */
+#define OPEN_WALL 0u
+#define OPEN_FREE 1u
+#define OPEN_NORMAL 2u
+#define OPEN_STAGE 3u
+#define OPEN_INFLOW 4u
+#define OPEN_NEWTON_STEPS 4
+
+/* x^(1/3) for x >= 0 by pow43's Newton sequence: GLSL's pow(x, 1/3) has no
+   fixed rounding, and this is a value it admits. */
+static float cbrt_newton(float x) {
+    if (!(x > 0.0f)) return 0.0f;
+    float r = bitsf(fbits(x) / 3u + 0x2A555555u);
+    for (int k = 0; k < 4; ++k) r = (2.0f * r + x / (r * r)) / 3.0f;
+    return r;
+}
+
+static uint32_t open_kind(const oracle_t *o, int cR) { return o->open_cond[2u * (uint32_t)(-2 - cR)]; }
+static float open_value(const oracle_t *o, int cR) { return bitsf(o->open_cond[2u * (uint32_t)(-2 - cR) + 1u]); }
+
+static int open_forced(const oracle_t *o, int cR) {
+    return cR < -1 && open_kind(o, cR) == OPEN_INFLOW && open_value(o, cR) > 0.0f;
+}
+
+/* hG solving -q/hG + 2 sqrt(g hG) = riemann, Newton in s = sqrt(hG). */
+static float inflow_depth(const oracle_t *o, float q, float riemann) {
+    float root_g = sqrtf(o->g);
+    float s = gmax(cbrt_newton(q / (2.0f * root_g)), riemann / (2.0f * root_g));
+    for (int k = 0; k < OPEN_NEWTON_STEPS; ++k) {
+        float f = 2.0f * root_g * s - q / (s * s) - riemann;
+        float df = 2.0f * root_g + 2.0f * q / (s * s * s);
+        s = gmax(s - f / df, 0.5f * s);
+    }
+    return s * s;
+}
+
+static void ghost_state(const oracle_t *o, uint32_t kind, float value, float hL, float huL, float hvL, float nx_,
+                        float ny_, float *hG, float *huG, float *hvG) {
+    float uL = safe_vel(o, hL, huL);
+    float vL = safe_vel(o, hL, hvL);
+    float unL = uL * nx_ + vL * ny_;
+    float ut = -uL * ny_ + vL * nx_;
+    float cL = sqrtf(o->g * gmax(hL, 0.0f));
+    float un = -unL;
+    *hG = hL;
+    if (kind == OPEN_FREE) {
+        un = fabsf(unL);
+    } else if (kind == OPEN_NORMAL) {
+        float r = cbrt_newton(gmax(hL, 0.0f));
+        un = value * (r * r);
+    } else if (kind == OPEN_STAGE) {
+        if (hL < o->dry_tol || unL < cL) {
+            *hG = value;
+            un = unL + 2.0f * (cL - sqrtf(o->g * value));
+        } else {
+            un = unL;
+        }
+    } else if (kind == OPEN_INFLOW && value > 0.0f) {
+        *hG = inflow_depth(o, value, unL + 2.0f * cL);
+        un = -value / *hG;
+        ut = 0.0f;
+    }
+    *huG = *hG * (un * nx_ - ut * ny_);
+    *hvG = *hG * (un * ny_ + ut * nx_);
+}
+
+static float boundary_mass_flux(uint32_t kind, float value, float Fh) {
+    if (kind == OPEN_FREE || kind == OPEN_NORMAL) return gmax(Fh, 0.0f);
+    if (kind == OPEN_STAGE) return Fh;
+    if (kind == OPEN_INFLOW) return -value;
+    return 0.0f;
+}
+
+/* The ghost probe of the reference's tests: per case (h, hu, hv, nx, ny, flux)
+   and condition words, the ghost (h, hu, hv) and the boundary mass flux. */
+void oracle_open_ghost(float g, float dry_tol, const float *cases, const uint32_t *cond, float *results, uint32_t n) {
+    oracle_t o;
+    memset(&o, 0, sizeof o);
+    o.g = g;
+    o.dry_tol = dry_tol;
+    for (uint32_t k = 0; k < n; ++k) {
+        const float *c = cases + 6u * k;
+        float *r = results + 4u * k;
+        float value = bitsf(cond[2u * k + 1u]);
+        ghost_state(&o, cond[2u * k], value, c[0], c[1], c[2], c[3], c[4], &r[0], &r[1], &r[2]);
+        r[3] = boundary_mass_flux(cond[2u * k], value, c[5]);
+    }
+}
+
 static inline int block_active(const oracle_t *o, uint32_t b) { return o->blk[BLK_WORDS * b + BLK_ACTIVE] != 0u; }
 
 static void load_state(const oracle_t *o, int stage, int c, float *h_, float *hu_, float *hv_) {
@@ -226,15 +325,31 @@ void oracle_flux_stage(oracle_t *o, int stage) {
                 hR = hL;
                 huR = huL - 2.0f * (huL * nx_ + hvL * ny_) * nx_;
                 hvR = hvL - 2.0f * (huL * nx_ + hvL * ny_) * ny_;
+            } else if (cR < 0) {
+                ghost_state(o, open_kind(o, cR), open_value(o, cR), hL, huL, hvL, nx_, ny_, &hR, &huR, &hvR);
             } else {
                 load_state(o, stage, cR, &hR, &huR, &hvR);
             }
-            if (hL < o->dry_tol && hR < o->dry_tol) continue;
+            if (hL < o->dry_tol && hR < o->dry_tol && !open_forced(o, cR)) {
+                /* an open edge clears its words instead, as the gather reads them */
+                if (cR < -1) memset(o->ef + EF_WORDS * eid, 0, EF_WORDS * sizeof(float));
+                continue;
+            }
             float dzL = o->edz[2u * eid], dzR = o->edz[2u * eid + 1u];
             float hLs, hqnL, hqtL, hRs, hqnR, hqtR, Fh, Fhn, Fht, Smax;
             face_states(o, hL, huL, hvL, dzL, hR, huR, hvR, dzR, nx_, ny_, &hLs, &hqnL, &hqtL, &hRs, &hqnR, &hqtR);
             hllc(o, hLs, hqnL, hqtL, hRs, hqnR, hqtR, &Fh, &Fhn, &Fht, &Smax);
-            if (cR < 0) Fh = 0.0f; /* a wall passes no mass */
+            if (cR < -1 && (open_kind(o, cR) == OPEN_FREE || open_kind(o, cR) == OPEN_NORMAL) && Fh < 0.0f) {
+                /* an outflow-only edge drawing water in is a wall for this stage, momentum included */
+                ghost_state(o, OPEN_WALL, 0.0f, hL, huL, hvL, nx_, ny_, &hR, &huR, &hvR);
+                face_states(o, hL, huL, hvL, dzL, hR, huR, hvR, dzR, nx_, ny_, &hLs, &hqnL, &hqtL, &hRs, &hqnR, &hqtR);
+                hllc(o, hLs, hqnL, hqtL, hRs, hqnR, hqtR, &Fh, &Fhn, &Fht, &Smax);
+                Fh = 0.0f;
+            } else if (cR < -1) {
+                Fh = boundary_mass_flux(open_kind(o, cR), open_value(o, cR), Fh);
+            } else if (cR < 0) {
+                Fh = 0.0f; /* a wall passes no mass */
+            }
             float Fhu = Fhn * nx_ - Fht * ny_;
             float Fhv = Fhn * ny_ + Fht * nx_;
             float SL_g = 0.5f * o->g * (hL * hL - hLs * hLs);
@@ -249,6 +364,27 @@ void oracle_flux_stage(oracle_t *o, int stage) {
             w[4] = Fhv * len + SR_g * ny_ * len;
             if (stage) w[EF_CFL] = Smax * len;
         }
+    }
+}
+
+/* Volume through every open edge after one flux stage: dt/2 of its mass word
+   into its out or in pair, skipping edges whose block is inactive (their
+   words are stale). */
+void oracle_tally(oracle_t *o) {
+    if (o->dt_buf[0] == 0u || !o->open_vol) return;
+    float half_dt = 0.5f * bitsf(o->dt_buf[0]);
+    for (uint32_t e = 0; e < o->E; ++e) {
+        int cR = o->ecR[e];
+        if (cR >= -1) continue;
+        if (!block_active(o, (uint32_t)o->ecL[e] >> 8)) continue;
+        float v = half_dt * o->ef[EF_WORDS * e];
+        float *t = o->open_vol + 4u * (uint32_t)(-2 - cR) + ((v < 0.0f) ? 2u : 0u);
+        float s, err, hi, lo;
+        two_sum(t[0], fabsf(v), &s, &err);
+        err += t[1];
+        two_sum(s, err, &hi, &lo);
+        t[0] = hi;
+        t[1] = lo;
     }
 }
 
@@ -433,6 +569,8 @@ void oracle_cfl_prologue(oracle_t *o) {
             hR = hL;
             huR = huL - 2.0f * (huL * nx_ + hvL * ny_) * nx_;
             hvR = hvL - 2.0f * (huL * nx_ + hvL * ny_) * ny_;
+        } else if (cR < 0) {
+            ghost_state(o, open_kind(o, cR), open_value(o, cR), hL, huL, hvL, nx_, ny_, &hR, &huR, &hvR);
         } else { hR = o->h[cR]; huR = o->hu[cR]; hvR = o->hv[cR]; }
         float contrib = 0.0f;
         if (hL >= o->dry_tol || hR >= o->dry_tol)
@@ -479,6 +617,7 @@ void oracle_step(oracle_t *o, const uint32_t *src_cells, const float *src_rate, 
                  int track_clamp, int active_set) {
     for (int stage = 0; stage < 2; ++stage) {
         oracle_flux_stage(o, stage);
+        oracle_tally(o);
         oracle_update_stage(o, stage, compensated, track_clamp);
     }
     if (n_src) oracle_sources(o, src_cells, src_rate, n_src, compensated);

@@ -11,7 +11,11 @@ drives its shaders:
 * ``_set_sources`` (``:529-560``): nonzero cells as (cell, rate / area);
 * ``_record_prologue`` (``:567-591``), ``_record_step`` (``:489-513``) and the
   window loop of ``run`` (``:609-762``), with ``steps_per_graph`` steps per
-  submit and the control block read back after each.
+  submit and the control block read back after each;
+* open boundaries as ``SWESolver`` numbers them (``inundation/vulkan/solver.py:236-243``,
+  open edge k has right cell ``-2 - k`` in stretch order), their conditions and
+  forced blocks (``gpu_resident_batch.py:447-458``) and the volume through each
+  stretch (``solver.py:432-440``).
 """
 
 from __future__ import annotations
@@ -101,7 +105,7 @@ class _Oracle(ctypes.Structure):
         *[(name, ctypes.c_void_p) for name in (
             "ecL", "ecR", "enx", "eny", "elen", "edz", "area", "n_mann", "cptr", "cidx", "erange", "bptr", "bidx",
             "h", "hu", "hv", "h1", "hu1", "hv1", "h_lo", "h1_lo", "ef", "touched", "blk", "dt_buf", "clamp_mass", "ctrl",
-            "src_hydro", "src_hscale", "knot_ptr", "knot_t", "knot_q",
+            "src_hydro", "src_hscale", "knot_ptr", "knot_t", "knot_q", "open_cond", "open_vol",
         )],
     ]
 
@@ -128,6 +132,7 @@ class ResidentOracle:
     track_clamp: bool = False
     cfl_safety: float = 1.0
     steps_total: int = 0
+    open_edges: tuple = ()
     arrays: dict = field(default_factory=dict)
 
     def __post_init__(self) -> None:
@@ -136,8 +141,15 @@ class ResidentOracle:
         self.cfl = float(CFL_DEFAULT if self.cfl is None else self.cfl)
         order = edge_order_by_block(geom.edge_cellL, ACTIVE_BLOCK_CELLS)
         self.edge_order = order
+        self._open_stretches = [np.asarray(e, np.int64).ravel() for e in self.open_edges]
+        open_ids = np.concatenate([np.empty(0, np.int64), *self._open_stretches])
+        self.n_open = int(open_ids.size)
+        self._open_cells = geom.edge_cellL[open_ids].astype(np.int64)
+        cell_r = geom.edge_cellR.astype(np.int32).copy()
+        cell_r[open_ids] = -2 - np.arange(self.n_open, dtype=np.int32)
+        self.open_volume_snapshots: list[np.ndarray] = []
         ecl = geom.edge_cellL[order].astype(np.int32)
-        ecr = geom.edge_cellR[order].astype(np.int32)
+        ecr = cell_r[order]
         self.n_blocks = num_blocks(self.N)
         bptr, bidx = block_two_ring(*block_adjacency(ecl, ecr, self.N, ACTIVE_BLOCK_CELLS))
         f32 = np.float32
@@ -163,10 +175,15 @@ class ResidentOracle:
         a["touched"] = np.zeros(self.N, np.uint32)
         a["blk"] = np.zeros(3 * max(self.n_blocks, 1), np.uint32)
         a["dt_buf"] = np.array([0, 0x7149F2CA, 0, 0], np.uint32)
+        a["open_cond"] = np.zeros(2 * max(self.n_open, 1), np.uint32)
+        a["open_vol"] = np.zeros(4 * max(self.n_open, 1), np.float32)
         self.ctrl = np.zeros(1, CTRL_DTYPE)
         self._struct = _Oracle(self.N, self.E, self.n_blocks, self.g, self.dry_tol, self.cfl)
         for name, arr in a.items():
             setattr(self._struct, name, _ptr(arr))
+        if not self.n_open:
+            self._struct.open_cond = None
+            self._struct.open_vol = None
         self._struct.ctrl = _ptr(self.ctrl)
         self._sp = ctypes.byref(self._struct)
         self._src_cells = np.zeros(1, np.uint32)
@@ -202,6 +219,36 @@ class ResidentOracle:
         a["hv"][:] = self.hv0
         a["h_lo"][:] = 0.0
         a["h1_lo"][:] = 0.0
+        a["open_vol"][:] = 0.0
+
+    # -- open boundaries ---------------------------------------------------------------
+    def set_open_conditions(self, kinds: np.ndarray, values: np.ndarray) -> None:
+        """Every open edge's condition in stretch order; blocks an inflow or stage can wet stay forced."""
+        kinds = np.asarray(kinds, np.uint32).ravel()
+        values = np.asarray(values, np.float32).ravel()
+        if kinds.size != self.n_open or values.size != self.n_open:
+            raise ValueError(f"expected {self.n_open} open edges, got {kinds.size} kinds and {values.size} values")
+        words = self.arrays["open_cond"]
+        words[0 : 2 * self.n_open : 2] = kinds
+        words[1 : 2 * self.n_open : 2] = values.view(np.uint32)
+        blk = self.arrays["blk"]
+        blk[2::3] = 0
+        brings_water = np.isin(kinds, (3, 4)) & (values > 0.0)
+        blk[3 * (self._open_cells[brings_water] // ACTIVE_BLOCK_CELLS) + 2] = 1
+
+    def download_open_volumes(self) -> np.ndarray:
+        """``(stretches, 2)`` volume out of and into the mesh since the start, float64."""
+        if not self._open_stretches:
+            return np.zeros((0, 2), np.float64)
+        pairs = self.arrays["open_vol"][: 4 * self.n_open].astype(np.float64).reshape(-1, 4)
+        per_edge = np.column_stack([pairs[:, 0] + pairs[:, 1], pairs[:, 2] + pairs[:, 3]])
+        sizes = [e.size for e in self._open_stretches]
+        out = np.zeros((len(sizes), 2), np.float64)
+        o = 0
+        for s, n in enumerate(sizes):
+            out[s] = per_edge[o : o + n].sum(axis=0)
+            o += n
+        return out
 
     # -- kernels --------------------------------------------------------------------
     def set_sources(self, source_rate: np.ndarray | None, hydrographs: list | None = None) -> None:
@@ -291,9 +338,11 @@ class ResidentOracle:
         interval = seconds_to_ticks(output_interval_s)
         if not resume:
             self.reset()
+            self.open_volume_snapshots = []
         self.set_sources(source_rate, hydrographs)
         snaps = [self.download_h()]
         times = [ticks_to_seconds(start)]
+        self._capture_open()
         c = self.ctrl
         c["now_ticks"] = start
         c["steps"] = 0
@@ -320,18 +369,25 @@ class ResidentOracle:
             if not np.isfinite(h).all():
                 snaps.append(np.nan_to_num(h, nan=0.0, posinf=0.0))
                 times.append(ticks_to_seconds(stop))
+                self._capture_open()
                 finite = False
                 break
             if (stop - start) % interval == 0:
                 snaps.append(h)
                 times.append(ticks_to_seconds(stop))
+                self._capture_open()
         self.steps_total += int(c["steps"][0])
         if finite:
             h = self.download_h()
             if not np.allclose(snaps[-1], h):
                 snaps.append(h)
                 times.append(ticks_to_seconds(int(c["now_ticks"][0])))
+                self._capture_open()
         return snaps, times
+
+    def _capture_open(self) -> None:
+        if self.n_open:
+            self.open_volume_snapshots.append(self.download_open_volumes())
 
 
 def pow43(x: float) -> float:
@@ -370,3 +426,17 @@ def math_ok() -> bool:
     lib().oracle_two_sum(ctypes.c_float(1.0), ctypes.c_float(1e-9), ctypes.c_void_p(_ptr(se)))
     return float(se[1]) == float(np.float32(1e-9))
 
+
+
+def open_ghost_f32(g: float, dry_tol: float, cases: np.ndarray, kinds: np.ndarray, values: np.ndarray) -> np.ndarray:
+    """Rows of (h, hu, hv, nx, ny, HLLC mass flux) under open conditions -> rows of the
+    ghost (h, hu, hv) and the boundary mass flux, in float32 (the probe of the
+    reference's ``tests/unit/test_gpu_open_ghost.py``)."""
+    cases = np.ascontiguousarray(cases, np.float32).reshape(-1, 6)
+    cond = np.zeros((cases.shape[0], 2), np.uint32)
+    cond[:, 0] = np.asarray(kinds, np.uint32).ravel()
+    cond[:, 1] = np.asarray(values, np.float32).ravel().view(np.uint32)
+    out = np.zeros((cases.shape[0], 4), np.float32)
+    lib().oracle_open_ghost(ctypes.c_float(g), ctypes.c_float(dry_tol), ctypes.c_void_p(_ptr(cases)),
+                            ctypes.c_void_p(_ptr(cond)), ctypes.c_void_p(_ptr(out)), ctypes.c_uint32(cases.shape[0]))
+    return out

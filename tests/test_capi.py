@@ -67,8 +67,9 @@ def test_status_strings_and_argument_checks(lib: ctypes.CDLL) -> None:
 
 
 def test_ctypes_structs_match_the_header_layout() -> None:
-    assert ctypes.sizeof(native.SweMesh) == 16 + 17 * 8 + 8 + 11 * 8
-    assert ctypes.sizeof(native.SweState) == 17 * 8
+    assert ctypes.sizeof(native.SweMesh) == 16 + 17 * 8 + 8 + 11 * 8 + 8 + 8  # n_open (padded), open_cond
+    assert native.SweMesh.n_open.offset == 248 and native.SweMesh.open_cond.offset == 256
+    assert ctypes.sizeof(native.SweState) == 18 * 8
     assert ctypes.sizeof(native.SweParams) == 32
     assert ctypes.sizeof(native.SweSources) == 7 * 8 + 8
 
