@@ -51,7 +51,7 @@ OPEN_INFLOW = 4
 B200_BACKEND = "b200_resident"
 SOLVER_IMPLS = frozenset({"baseline", "fixed_dt_batch_barrier", "gpu_resident_batch", B200_BACKEND})
 MOMENTUM_SNAPSHOT_BACKENDS = frozenset({"baseline", "gpu_resident_batch", B200_BACKEND})
-OPEN_BOUNDARY_BACKENDS = frozenset({"baseline", "gpu_resident_batch"})
+OPEN_BOUNDARY_BACKENDS = frozenset({"baseline", "gpu_resident_batch", B200_BACKEND})
 
 
 def float_bits(value: float) -> int:

@@ -8,8 +8,13 @@ Vulkan backends (``baseline``, ``fixed_dt_batch_barrier``,
 ``gpu_resident_batch``) are accepted by the config, as in the reference, and
 refused by ``prepare()``: this package has no Vulkan path.
 
-Not carried over: open boundaries (``open_boundaries`` must be empty for
-``b200_resident``) and the GIS mesh readers (meshes come from a geometry-cache
+Open boundaries work as in the reference (``workflow.py:361-445, 789-806,
+859-867, 947-953``): each ``OpenBoundary`` line selects its stretch of wall
+edges at ``prepare()``, every phase names a condition for every stretch, and
+``WorkflowResult.boundary_volumes_m3`` holds each stretch's cumulative volume
+out of and into the mesh at every snapshot.
+
+Not carried over: the GIS mesh readers (meshes come from a geometry-cache
 artifact, an ``.obj`` or an ``.npz`` file, or a ``MeshGeometry`` passed in).
 """
 
@@ -21,15 +26,29 @@ import time
 from collections.abc import Mapping, Sequence
 from dataclasses import dataclass, field
 from pathlib import Path
+from dataclasses import astuple
 from typing import Any, Literal
 
 import numpy as np
 from numpy.typing import NDArray
 
+from .mesh.boundaries import conveyance_split, select_boundary_edges
 from .mesh.cache import geometry_cache_key, load_geometry_cache, load_geometry_cache_artifact, save_geometry_cache
 from .mesh.geometry import MeshGeometry, build_geometry, hilbert_reorder
 from .mesh.loader import load_mesh_file
-from .tuning import B200_BACKEND, DRY_TOL_DEFAULT, GRAVITY_G, MOMENTUM_SNAPSHOT_BACKENDS, OPEN_BOUNDARY_BACKENDS, SOLVER_IMPLS
+from .tuning import (
+    B200_BACKEND,
+    DRY_TOL_DEFAULT,
+    GRAVITY_G,
+    MOMENTUM_SNAPSHOT_BACKENDS,
+    OPEN_BOUNDARY_BACKENDS,
+    OPEN_FREE,
+    OPEN_INFLOW,
+    OPEN_NORMAL,
+    OPEN_STAGE,
+    OPEN_WALL,
+    SOLVER_IMPLS,
+)
 
 INITIAL_STATE_METADATA_KEYS = frozenset({"saved_order", "mesh_source", "t_end_s", "dt_max", "cfl_interval"})
 
@@ -336,6 +355,62 @@ def load_initial_state(source, n_cells: int, zb: NDArray[np.float32], *, order: 
     return h, hu, hv, n_mann
 
 
+def open_stretch_edges(geom: MeshGeometry, boundaries: Sequence[OpenBoundary]) -> list[NDArray[np.int64]]:
+    """Each stretch's wall edges (``workflow.py:361-377``); a stretch selecting none, or an edge twice, raises."""
+    stretches = [select_boundary_edges(geom, b.line, b.tolerance_m) for b in boundaries]
+    for b, edges in zip(boundaries, stretches, strict=True):
+        if not edges.size:
+            raise ValueError(f"open boundary {b.name!r} selects no boundary edges within {b.tolerance_m} m of its line")
+    every = np.concatenate(stretches) if stretches else np.empty(0, dtype=np.int64)
+    if np.unique(every).size != every.size:
+        raise ValueError("open boundaries select the same edge twice")
+    return stretches
+
+
+def open_conditions(geom: MeshGeometry, manning: NDArray[np.float32], boundary: OpenBoundary,
+                    condition: BoundaryCondition, edges: NDArray[np.int64]) -> tuple[int, NDArray[np.float32]]:
+    """Condition code and per-edge value of one stretch (``workflow.py:380-412``).
+
+    Normal depth: sqrt(S) / n of the cell inside; stage: the level's depth over
+    that cell's bed (0 below it); inflow: discharge per unit width by conveyance.
+    """
+    cells = geom.edge_cellL[edges]
+    if not np.isfinite(astuple(condition)).all():
+        raise ValueError(f"open boundary {boundary.name!r} has a non-finite value: {condition}")
+    if isinstance(condition, Wall):
+        return OPEN_WALL, np.zeros(edges.size, dtype=np.float32)
+    if isinstance(condition, FreeOutflow):
+        return OPEN_FREE, np.zeros(edges.size, dtype=np.float32)
+    if isinstance(condition, NormalDepth):
+        if condition.energy_slope <= 0.0:
+            raise ValueError(f"open boundary {boundary.name!r} needs a positive energy slope")
+        return OPEN_NORMAL, (np.sqrt(condition.energy_slope) / manning[cells]).astype(np.float32)
+    if isinstance(condition, Stage):
+        depth = condition.elevation_m - geom.zb[cells].astype(np.float64)
+        return OPEN_STAGE, np.maximum(depth, 0.0).astype(np.float32)
+    if condition.energy_slope <= 0.0:
+        raise ValueError(f"open boundary {boundary.name!r} needs a positive energy slope")
+    if condition.discharge_m3s < 0.0:
+        raise ValueError(f"open boundary {boundary.name!r} has a negative inflow")
+    return OPEN_INFLOW, conveyance_split(condition.discharge_m3s, geom.edge_len[edges], geom.zb[cells],
+                                         manning[cells], condition.energy_slope)
+
+
+def build_phase_open_conditions(geom: MeshGeometry, manning: NDArray[np.float32], boundaries: Sequence[OpenBoundary],
+                                stretches: Sequence[NDArray[np.int64]],
+                                phase: SimulationPhase) -> tuple[NDArray[np.uint32], NDArray[np.float32]]:
+    """Per-edge condition codes and values of one phase, in stretch order (``workflow.py:415-437``)."""
+    names = {b.name for b in boundaries}
+    if set(phase.boundaries) != names:
+        raise ValueError(f"phase boundaries {sorted(phase.boundaries)} must name every open boundary: {sorted(names)}")
+    kinds, values = [], []
+    for b, edges in zip(boundaries, stretches, strict=True):
+        kind, value = open_conditions(geom, manning, b, phase.boundaries[b.name], edges)
+        kinds.append(np.full(edges.size, kind, dtype=np.uint32))
+        values.append(value)
+    return np.concatenate(kinds), np.concatenate(values)
+
+
 def _backend_class(name: str):
     if name == B200_BACKEND:
         from .backend import SWESolverB200Resident
@@ -356,6 +431,8 @@ class SWEWorkflow:
         self.perm: NDArray[np.int32] | None = None
         self.solver: Any = None
         self._geometry = geometry
+        self._open_stretches: list[NDArray[np.int64]] = []
+        self._manning: NDArray[np.float32] | None = None
 
     def _log(self, msg: str) -> None:
         if self.config.progress:
@@ -396,8 +473,6 @@ class SWEWorkflow:
     def prepare(self) -> None:
         cfg = self.config
         cls = _backend_class(cfg.solver_impl)
-        if cfg.open_boundaries:
-            raise ValueError(f"{cfg.solver_impl} does not support open boundaries yet")
         geom, perm = self._load_geometry()
         h0 = np.zeros(geom.N, dtype=np.float32)
         hu0 = np.zeros(geom.N, dtype=np.float32)
@@ -411,8 +486,11 @@ class SWEWorkflow:
             h0, hu0, hv0, n_loaded = loaded
             if n_loaded is not None:
                 n0 = n_loaded
+        self._open_stretches = open_stretch_edges(geom, cfg.open_boundaries)
+        self._manning = np.asarray(n0, dtype=np.float32)
+        open_args: dict[str, Any] = {"open_edges": self._open_stretches} if self._open_stretches else {}
         solver = cls(geom, None, h0, hu0, hv0, n0, g=cfg.gravity, dry_tol=cfg.dry_tol, cfl=cfg.cfl,
-                     workgroup_size=cfg.workgroup_size)
+                     workgroup_size=cfg.workgroup_size, **open_args)
         if cfg.track_clamp_mass:
             solver.track_clamp = True
         if cfg.steps_per_graph is not None:
@@ -441,9 +519,10 @@ class SWEWorkflow:
         for k, phase in enumerate(phases):
             if phase.duration_s <= 0.0:
                 raise ValueError(f"Phase {k} has non-positive duration.")
-            if phase.boundaries:
-                raise ValueError(f"{cfg.solver_impl} does not support open boundaries yet")
             t_end = t + phase.duration_s
+            if self._open_stretches:
+                self.solver.set_open_conditions(*build_phase_open_conditions(
+                    self.geom, self._manning, cfg.open_boundaries, self._open_stretches, phase))
             out = self.solver.run(
                 t_end=t_end, output_interval_s=cfg.output_interval_s, dt_max=cfg.dt_max, dt_init=cfg.dt_init,
                 progress=cfg.progress, source_rate=build_phase_source_rate(self.geom, phase, valid), resume=k > 0,
@@ -466,11 +545,15 @@ class SWEWorkflow:
         clamp = None
         if cfg.track_clamp_mass:
             clamp = float(np.asarray(self.solver.download_clamp_mass(), dtype=np.float64).sum())
+        volumes: dict[str, NDArray[np.float64]] = {}
+        if self._open_stretches:
+            stacked = np.stack(self.solver.open_volume_snapshots)
+            volumes = {b.name: stacked[:, k] for k, b in enumerate(cfg.open_boundaries)}
         return WorkflowResult(
             snapshots=snaps, snap_times=times, h_final=h_final, volume_final_m3=volume,
             volume_injected_m3=injected, wall_seconds=wall, steps_total=int(self.solver.steps_total),
             hu_final=self.solver.download_hu(), hv_final=self.solver.download_hv(), hu_snapshots=hu_s,
-            hv_snapshots=hv_s, clamp_mass_m3=clamp,
+            hv_snapshots=hv_s, clamp_mass_m3=clamp, boundary_volumes_m3=volumes,
         )
 
 
@@ -493,6 +576,7 @@ def inflow_phases(upstream: WorkflowResult, outlet: str, into: str, energy_slope
 
 __all__ = [
     "BoundaryCondition", "FreeOutflow", "Inflow", "NormalDepth", "OpenBoundary", "PointSource", "SWEWorkflow",
-    "SimulationPhase", "Stage", "Wall", "WorkflowConfig", "WorkflowResult", "build_phase_source_rate",
-    "inflow_phases", "load_initial_state", "select_cells_within_radius",
+    "SimulationPhase", "Stage", "Wall", "WorkflowConfig", "WorkflowResult", "build_phase_open_conditions",
+    "build_phase_source_rate", "inflow_phases", "load_initial_state", "open_conditions", "open_stretch_edges",
+    "select_cells_within_radius",
 ]
