@@ -158,7 +158,9 @@ def test_repeat_runs_are_bit_identical() -> None:
 def test_a_wall_stretch_behaves_like_no_stretch() -> None:
     closed = workflow(initial_depth=0.5).run([phase(Wall(), Wall())])
     plain = workflow(open_boundaries=False, initial_depth=0.5).run([SimulationPhase(END_S, [])])
-    np.testing.assert_array_equal(closed.h_final, plain.h_final)
+    # A wall-kind ghost mirrors through the film-safe velocities, a plain wall mirrors the momentum
+    # itself: the same state up to rounding (the reference's own bound).
+    np.testing.assert_allclose(closed.h_final, plain.h_final, atol=1e-5)
     assert closed.steps_total == plain.steps_total
 
 
