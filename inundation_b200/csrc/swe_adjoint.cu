@@ -610,7 +610,7 @@ __global__ void __launch_bounds__(kThreads)
     extern __shared__ float4 smem4[];
     float *G = reinterpret_cast<float *>(smem4);
     __shared__ int flag[2];
-    GridSync g{a.sync, a.sync + 32, 0u};
+    GridSync g{a.sync, a.sync + 32, 0u, 0u};
     if (threadIdx.x == 0) g.epoch = ld_acquire_u32(g.gen);
     __syncthreads();
     const uint32_t n = m.n_blocks * kBlockCells;

@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(kPersistThreads, 1024 / kPersistThreads)
     __shared__ TiledShared<kPersistThreads> sh;
     __shared__ int flag[2];
     __shared__ uint32_t epoch0;
-    GridSync g{s.sync, s.sync + 32, 0u};
+    GridSync g{s.sync, s.sync + 32, 0u, 0u};
     if (threadIdx.x == 0) {
         mbar_init(reinterpret_cast<uint64_t *>(smem), 1u);
         mbar_init(reinterpret_cast<uint64_t *>(smem) + 1, 1u);
@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(kPersistThreads, 1024 / kPersistThreads)
                 s.dt_buf[kDtWords * i + 2u] = s.dt_buf[kDtWords * i];
                 step_control(s.ctrl + i, s.dt_buf + kDtWords * i, 1);
             }
-            if (threadIdx.x == 0) {
+            if (threadIdx.x == blockDim.x - 1u) {  // beside instance 0's control, not after it
                 volatile uint32_t *sched = s.sched;
                 sched[kSchedPrevActive] = sched[kSchedActive];
                 sched[kSchedActive] = sched[kSchedNext];

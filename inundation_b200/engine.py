@@ -408,6 +408,7 @@ class ResidentEngine:
             self._sched[:3].zero_()  # list counters and epoch; words 6-7 keep the computed-cells total
             self._sched[4:].zero_()
             self._marks.zero_()
+            self._sync.zero_()  # barrier counters: consistent again even after a launch that stopped on a timeout
             native.check(
                 self._lib.swe_prologue(
                     ctypes.byref(self._mesh), ctypes.byref(self._state), ctypes.byref(p), self._cuda_stream
