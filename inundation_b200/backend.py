@@ -82,6 +82,7 @@ class SWESolverB200Resident(ResidentEngine):
         self.geom = geom
         self.N, self.E = int(geom.N), int(geom.E)
         self.steps_total = 0
+        self._pinned: dict[str, torch.Tensor] = {}
         self._open_stretches = [np.asarray(edges, dtype=np.int64).ravel() for edges in open_edges]
         # (stretches, 2) volume out of and into the mesh at every snapshot of a run.
         self.open_volume_snapshots: list[NDArray[np.float64]] = []
@@ -111,28 +112,38 @@ class SWESolverB200Resident(ResidentEngine):
         self.reset(self._h0, self._hu0, self._hv0)
 
     # -- public state access (reference solver.py:390-497) --------------------------------------
-    def _download(self, tensor: torch.Tensor) -> NDArray[np.float32]:
+    def _staging(self, name: str) -> torch.Tensor:
+        """A page-locked host array of N floats, one per purpose, kept for the solver's life."""
+        buf = self._pinned.get(name)
+        if buf is None:
+            buf = torch.empty(self.N, dtype=torch.float32).pin_memory()
+            self._pinned[name] = buf
+        return buf
+
+    def _download(self, name: str) -> NDArray[np.float32]:
+        buf = self._staging("down")
         with torch.cuda.stream(self._stream):
-            out = tensor[: self.N].cpu().numpy()
-        return out.copy()
+            buf.copy_(self._t[name][: self.N], non_blocking=True)
+        self._stream.synchronize()
+        return buf.numpy().copy()
 
     def download_h(self) -> NDArray[np.float32]:
-        return self._download(self._t["h"])
+        return self._download("h")
 
     def download_hu(self) -> NDArray[np.float32]:
-        return self._download(self._t["hu"])
+        return self._download("hu")
 
     def download_hv(self) -> NDArray[np.float32]:
-        return self._download(self._t["hv"])
+        return self._download("hv")
 
     def download_h_residual(self) -> NDArray[np.float32]:
-        return self._download(self._t["h_lo"])
+        return self._download("h_lo")
 
     def download_h_precise(self) -> NDArray[np.float64]:
         return self.download_h().astype(np.float64) + self.download_h_residual().astype(np.float64)
 
     def download_clamp_mass(self) -> NDArray[np.float32]:
-        return self._download(self._t["clamp_mass"])
+        return self._download("clamp_mass")
 
     def reset_clamp_mass(self) -> None:
         with torch.cuda.stream(self._stream):
@@ -146,18 +157,26 @@ class SWESolverB200Resident(ResidentEngine):
         self._stream.synchronize()
 
     def reset(self, h0: NDArray[np.float32], hu0: NDArray[np.float32], hv0: NDArray[np.float32]) -> None:
-        """Upload initial conditions; the compensated low words start at zero."""
-        self._h0 = np.asarray(h0, np.float32).ravel().copy()
-        self._hu0 = np.asarray(hu0, np.float32).ravel().copy()
-        self._hv0 = np.asarray(hv0, np.float32).ravel().copy()
+        """Upload initial conditions; the compensated low words start at zero.
+
+        The initial state is kept in page-locked host arrays of the solver (one per
+        array), from which this and every later reset copy it asynchronously.
+        """
+        kept = []
         with torch.cuda.stream(self._stream):
-            self._t["h"][: self.N].copy_(torch.from_numpy(self._h0))
-            self._t["hu"][: self.N].copy_(torch.from_numpy(self._hu0))
-            self._t["hv"][: self.N].copy_(torch.from_numpy(self._hv0))
+            for name, values in (("h", h0), ("hu", hu0), ("hv", hv0)):
+                buf = self._staging("initial_" + name)
+                host = buf.numpy()
+                src = np.asarray(values, np.float32).ravel()
+                if src.ctypes.data != host.ctypes.data:  # a reset to the kept state copies nothing on the host
+                    host[:] = src
+                self._t[name][: self.N].copy_(buf, non_blocking=True)
+                kept.append(host)
             self._t["h_lo"].zero_()
             self._t["h1_lo"].zero_()
             self._open_vol.zero_()
         self._stream.synchronize()
+        self._h0, self._hu0, self._hv0 = kept
 
     def _reset_to_initial(self) -> None:
         self.reset(self._h0, self._hu0, self._hv0)
@@ -300,7 +319,7 @@ class SWESolverB200Resident(ResidentEngine):
         self.steps_total += int(ctrl["steps"][0])
         if finite:
             h_final = self.download_h()
-            if not np.allclose(snapshots[-1], h_final):
+            if not (np.array_equal(snapshots[-1], h_final) or np.allclose(snapshots[-1], h_final)):
                 snapshots.append(h_final)
                 snap_times.append(ticks_to_seconds(int(ctrl["now_ticks"][0])))
                 capture()
