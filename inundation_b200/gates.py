@@ -454,10 +454,13 @@ CASES: dict[str, Callable[[], dict]] = {
 
 def main(argv: list[str] | None = None) -> int:
     ap = argparse.ArgumentParser(description="physical validation gates of the B200 backend")
-    ap.add_argument("cases", nargs="*", default=list(CASES), choices=list(CASES))
+    ap.add_argument("cases", nargs="*", metavar="case", help=f"any of {', '.join(CASES)} (default: all)")
     args = ap.parse_args(argv)
+    unknown = sorted(set(args.cases) - set(CASES))
+    if unknown:
+        ap.error(f"unknown cases {unknown}; choose from {list(CASES)}")
     ok = True
-    for name in args.cases:
+    for name in args.cases or list(CASES):
         res = CASES[name]()
         ok &= res["passed"]
         print(json.dumps(res), flush=True)
