@@ -26,6 +26,11 @@ The cases and thresholds of the reference's benchmark harnesses
 * ``held_lake``: still water at 12 m over a bed of two sines, held by its own
   level as a stage at both ends, 300 s: level within 1e-4 m, speeds below
   1e-3 m/s.
+* ``backwater_m1`` / ``backwater_m2``: the inflow into a 3 km channel held at its
+  outlet 0.8 m or 0.25 m above the bed, 6 h, against the gradually varied flow
+  profile (within 1.5 %).
+* ``basins``: a hydrograph through a 4 km channel run whole, and cut in two with
+  the upper half's outflow passed into the lower half by ``inflow_phases``.
 
 ``python -m inundation_b200.gates [case ...]`` prints one JSON line per case.
 """
@@ -189,11 +194,45 @@ def _geometry(verts: NDArray, faces: NDArray, offsets: NDArray | None, zb: NDArr
 
 
 def channel_geometry(cells: int, across: int, length: float, width: float,
-                     bed: Callable[[NDArray], NDArray] | None = None) -> MeshGeometry:
+                     bed: Callable[[NDArray], NDArray] | None = None, x0: float = 0.0) -> MeshGeometry:
+    """A channel of ``cells`` x ``across`` rectangles from x = x0, its bed a function of x."""
     mesh = channel_grid(cells, across, length, width)
-    x = np.tile((np.arange(cells) + 0.5) * (length / cells), across)
+    x = np.tile((np.arange(cells) + 0.5) * (length / cells), across) + x0
     zb = np.zeros(x.size) if bed is None else bed(x)
-    return _geometry(mesh.verts, mesh.faces, mesh.offsets, zb)
+    verts = mesh.verts.copy()
+    verts[:, 0] += x0
+    return _geometry(verts, mesh.faces, mesh.offsets, zb)
+
+
+def column_profile(geom: MeshGeometry, h: NDArray) -> tuple[NDArray, NDArray]:
+    """Depth averaged across a channel, by position along it."""
+    x, inverse = np.unique(np.round(geom.world_centroid[:, 0], 6), return_inverse=True)
+    return x, np.bincount(inverse, weights=np.asarray(h, np.float64)) / np.bincount(inverse)
+
+
+def gradually_varied_profile(x: NDArray, depth_at_end: float, end_x: float, unit_discharge: float, slope: float,
+                             manning: float, g: float = GRAVITY_G) -> NDArray:
+    """Steady depth at ascending x, integrated upstream from ``end_x`` by classical RK4 steps
+    of at most 1 m on dh/dx = (S - Sf) / (1 - Fr^2), Sf = n^2 q^2 / h^(10/3), Fr^2 = q^2 / (g h^3)."""
+
+    def dhdx(h: float) -> float:
+        return (slope - manning**2 * unit_discharge**2 / h ** (10.0 / 3.0)) / (1.0 - unit_discharge**2 / (g * h**3))
+
+    out = np.empty(len(x))
+    h, pos = depth_at_end, end_x
+    for k in range(len(x) - 1, -1, -1):
+        dist = pos - float(x[k])
+        n = max(1, math.ceil(dist))
+        dx = -dist / n
+        for _ in range(n):
+            k1 = dhdx(h)
+            k2 = dhdx(h + 0.5 * dx * k1)
+            k3 = dhdx(h + 0.5 * dx * k2)
+            k4 = dhdx(h + dx * k3)
+            h += dx * (k1 + 2.0 * k2 + 2.0 * k3 + k4) / 6.0
+        out[k] = h
+        pos = float(x[k])
+    return out
 
 
 def square_geometry(n: int, side: float, origin: float = 0.0,
@@ -424,6 +463,103 @@ def held_lake(cells: int = 200, length: float = 1000.0, width: float = 40.0, acr
     return _verdict(out, {"level_error_m": 1e-4, "speed_max_ms": 1e-3}, strict=("level_error_m", "speed_max_ms"))
 
 
+def _workflow(geom: MeshGeometry, ends: list, *, output_interval_s: float, manning: float = 0.03):
+    from .workflow import SWEWorkflow, WorkflowConfig
+
+    wf = SWEWorkflow(WorkflowConfig(mesh_source="channel", manning_n=manning, output_interval_s=output_interval_s,
+                                    dt_max=5.0, cfl_interval=1, progress=False, track_clamp_mass=True,
+                                    open_boundaries=ends), geometry=geom)
+    wf.prepare()
+    return wf
+
+
+def _end(name: str, x: float, width: float, dx: float):
+    from .workflow import OpenBoundary
+
+    return OpenBoundary(name, [(x, 0.0), (x, width)], 0.25 * dx)
+
+
+def _balance_rel(result, initial: float = 0.0) -> float:
+    last = [v[-1] for v in result.boundary_volumes_m3.values()]
+    went_out, went_in = float(sum(v[0] for v in last)), float(sum(v[1] for v in last))
+    return abs(initial + went_in - went_out - result.volume_final_m3) / max(initial + went_in, 1e-30)
+
+
+def backwater(end_depth: float = 0.8, cells: int = 600, length: float = 3000.0, width: float = 40.0,
+              discharge: float = 10.0, slope: float = 1e-3, manning: float = 0.03, hours: float = 6.0) -> dict:
+    """``inundation/bench/open_boundary.py`` backwater case: an inflow into a sloped channel held at
+    its outlet by a stage ``end_depth`` over the bed (0.8 m: an M1 profile, 0.25 m: M2), against the
+    gradually varied flow profile: interior columns within 1.5 %, last window's outflow within 1e-3."""
+    from .workflow import Inflow, SimulationPhase, Stage
+
+    sloped = lambda x: 10.0 - slope * x  # noqa: E731
+    geom = channel_geometry(cells, 2, length, width, bed=sloped)
+    dx = length / cells
+    wf = _workflow(geom, [_end("up", 0.0, width, dx), _end("down", length, width, dx)],
+                   output_interval_s=hours * 3600.0 / 6.0, manning=manning)
+    t0 = time.perf_counter()
+    r = wf.run([SimulationPhase(hours * 3600.0, [], {"up": Inflow(discharge, slope),
+                                                      "down": Stage(float(sloped(length)) + end_depth)})])
+    wall = time.perf_counter() - t0
+    x, h = column_profile(geom, r.h_final)
+    ref = gradually_varied_profile(x, end_depth, length, discharge / width, slope, manning)
+    went_out = r.boundary_volumes_m3["down"][:, 0]
+    window = hours * 3600.0 / 6.0
+    out = {"case": f"backwater_{'m1' if end_depth > normal_depth(discharge, width, slope, manning) else 'm2'}",
+           "cells": geom.N, "steps": r.steps_total, "wall_s": wall,
+           "profile_error_rel": float((np.abs(h - ref) / ref)[1:-1].max()),
+           "discharge_error_rel": abs((went_out[-1] - went_out[-2]) / window / discharge - 1.0),
+           "balance_rel": _balance_rel(r)}
+    return _verdict(out, {"profile_error_rel": 0.015, "discharge_error_rel": 1e-3, "balance_rel": 1e-7},
+                    strict=("profile_error_rel", "discharge_error_rel", "balance_rel"))
+
+
+def basins(cells: int = 400, length: float = 4000.0, width: float = 40.0, slope: float = 1e-3,
+           phase_s: float = 900.0, discharges: tuple[float, ...] = (5.0, 10.0, 15.0, 20.0, 15.0, 10.0, 5.0, 5.0),
+           output_s: float = 60.0) -> dict:
+    """``inundation/bench/open_boundary.py`` basins case: one channel run whole, then cut in two and
+    run upstream first, its outflow passed into the lower half through ``inflow_phases``: the volume
+    passed arrives (1e-6), the lower half's depths match the whole run's (1 %), and so does its
+    outflow (2 %); both halves' balances close (1e-7)."""
+    from .workflow import Inflow, NormalDepth, SimulationPhase, inflow_phases
+
+    sloped = lambda x: 10.0 - slope * x  # noqa: E731
+    cut = 0.5 * length
+    dx = length / cells
+
+    def hydrograph(down: str) -> list:
+        return [SimulationPhase(phase_s, [], {"up": Inflow(q, slope), down: NormalDepth(slope)}) for q in discharges]
+
+    t0 = time.perf_counter()
+    whole_g = channel_geometry(cells, 2, length, width, bed=sloped)
+    whole = _workflow(whole_g, [_end("up", 0.0, width, dx), _end("down", length, width, dx)],
+                      output_interval_s=output_s).run(hydrograph("down"))
+    upper_g = channel_geometry(cells // 2, 2, cut, width, bed=sloped)
+    first = _workflow(upper_g, [_end("up", 0.0, width, dx), _end("cut", cut, width, dx)],
+                      output_interval_s=output_s).run(hydrograph("cut"))
+    lower_g = channel_geometry(cells // 2, 2, cut, width, bed=sloped, x0=cut)
+    second = _workflow(lower_g, [_end("from_upper", cut, width, dx), _end("down", length, width, dx)],
+                       output_interval_s=output_s).run(
+        inflow_phases(first, "cut", "from_upper", slope, {"down": NormalDepth(slope)}))
+    wall = time.perf_counter() - t0
+    passed = float(first.boundary_volumes_m3["cut"][-1, 0])
+    received = float(second.boundary_volumes_m3["from_upper"][-1, 1])
+    xl, hl = column_profile(lower_g, second.h_final)
+    xw, hw = column_profile(whole_g, whole.h_final)
+    shared = hw[np.searchsorted(xw, xl - 1e-6)]
+    wet = shared > 0.01
+    out_whole = float(whole.boundary_volumes_m3["down"][-1, 0])
+    out_lower = float(second.boundary_volumes_m3["down"][-1, 0])
+    out = {"case": "basins", "cells": whole_g.N, "steps": whole.steps_total + first.steps_total + second.steps_total,
+           "wall_s": wall, "volume_passed_m3": passed, "passed_error_rel": abs(received / passed - 1.0),
+           "depth_difference_rel": float((np.abs(hl - shared)[wet] / shared[wet]).max()),
+           "outflow_difference_rel": abs(out_lower / out_whole - 1.0),
+           "upper_balance_rel": _balance_rel(first), "balance_rel": _balance_rel(second)}
+    gates = {"passed_error_rel": 1e-6, "depth_difference_rel": 0.01, "outflow_difference_rel": 0.02,
+             "upper_balance_rel": 1e-7, "balance_rel": 1e-7}
+    return _verdict(out, gates, strict=tuple(gates))
+
+
 def _verdict(out: dict, gates: dict, strict: tuple[str, ...] = ()) -> dict:
     """``passed`` and the failed gates: a value above its gate fails (at or above for ``strict``)."""
     failed = []
@@ -449,6 +585,9 @@ CASES: dict[str, Callable[[], dict]] = {
     "lake": lake,
     "uniform": uniform,
     "held_lake": held_lake,
+    "backwater_m1": lambda: backwater(0.8),
+    "backwater_m2": lambda: backwater(0.25),
+    "basins": basins,
 }
 
 

@@ -62,3 +62,18 @@ def test_thacker_keeps_its_volume_and_moves_as_one_body() -> None:
 def test_normal_depth_carries_the_discharge() -> None:
     h = normal_depth(10.0, 40.0, 1e-3, 0.03)
     assert h ** (5.0 / 3.0) * math.sqrt(1e-3) / 0.03 * 40.0 == pytest.approx(10.0, rel=1e-12)
+
+
+def test_the_backwater_reference_holds_normal_depth() -> None:
+    from inundation_b200.gates import gradually_varied_profile
+
+    target = normal_depth(10.0, 40.0, 1e-3, 0.03)
+    x = np.linspace(100.0, 2900.0, 8)
+    np.testing.assert_allclose(gradually_varied_profile(x, target, 3000.0, 0.25, 1e-3, 0.03), target, rtol=1e-9)
+
+
+def test_the_backwater_reference_rises_towards_a_high_level() -> None:
+    from inundation_b200.gates import gradually_varied_profile
+
+    x = np.linspace(100.0, 2900.0, 8)
+    assert (np.diff(gradually_varied_profile(x, 0.8, 3000.0, 0.25, 1e-3, 0.03)) > 0.0).all()
