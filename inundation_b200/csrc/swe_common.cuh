@@ -36,7 +36,9 @@ constexpr int kSchedItems = 3;      // tile work items of the current step
 constexpr int kSchedNextItems = 4;  // tile work items appended by the dilation
 constexpr int kSchedComputed = 6;   // [6,7]: uint64 cells computed over real steps
 constexpr int kSchedEpoch = 10;     // steps of the persistent kernel since the run's prologue
-constexpr int kSchedPrevActive = 11;  // blocks of the previous step's list (persistent kernel)
+constexpr int kSchedStartTaken = 11;  // tiles of the start list taken (persistent kernel)
+constexpr int kSchedQProd = 12;       // [12, 13]: tiles queued for steps of each parity (persistent kernel)
+constexpr int kSchedQCons = 14;       // [14, 15]: tiles taken from those queues (persistent kernel)
 
 // A tile work item: x = tile | (real cells << 25), y = first edge record,
 // z = first local-CSR entry, w = edge count | (padded slot count << 11) | (instance << 22).

@@ -13,6 +13,8 @@ namespace swe {
 
 
 // The compensated Heun update of one cell from its gathered sums (resident.py:354-513).
+// keep != nullptr: the new state also goes to shared memory at keep[0], keep[64],
+// keep[128], keep[192] (h, hu, hv, h_lo): the predictor's, or the committed one.
 template <int STAGE, bool COMP, bool CLAMP>
 __device__ __forceinline__ void update_cell(const swe_state_t &s, const Phys &p, float cfl, float dt, uint32_t i,
                                             float A, float n, float hi, float hui, float hvi, float loi, float h0,
@@ -61,9 +63,9 @@ __device__ __forceinline__ void update_cell(const swe_state_t &s, const Phys &p,
         }
         return;
     }
-    float hf;
+    float hf, lof = 0.0f;
     if (COMP) {
-        float sm, em, lof;
+        float sm, em;
         two_sum(h0, h_new, sm, em);
         em += lo0 + lo_new;
         two_sum(0.5f * sm, 0.5f * em, hf, lof);
@@ -80,6 +82,12 @@ __device__ __forceinline__ void update_cell(const swe_state_t &s, const Phys &p,
     }
     s.hu[i] = huf;
     s.hv[i] = hvf;
+    if (keep) {
+        keep[0] = hf;
+        keep[kTileCells] = huf;
+        keep[2 * kTileCells] = hvf;
+        keep[3 * kTileCells] = lof;
+    }
     wet = hf >= p.dry_tol;
     if (lam > 1e-30f && A > 1e-10f) bound = __float_as_uint(cfl * A / lam);
 }
@@ -299,9 +307,11 @@ __host__ __device__ inline size_t tiled_smem_bytes(uint32_t max_edges, uint32_t 
 // columns in_col..in_col+3 of B.c (h, hu, hv, h_lo), the committed state of the
 // corrector in com_col..com_col+3. F == nullptr: the flux words overwrite the
 // consumed records; otherwise they go to F (7 x capE words) and the records stay.
+// keep_pred: the new state also goes to columns 6..9 (predictor) or 0..3
+// (corrector). Returns, in the corrector, whether a cell of the tile is wet.
 // OPEN: the mesh has open edges (right cell -2 - k), with ghosts and tallies.
 template <int STAGE, bool COMP, bool CLAMP, int TPB, bool OPEN>
-__device__ __forceinline__ void tile_compute(const swe_mesh_t &m, const swe_state_t &s, const Phys &p, float cfl,
+__device__ __forceinline__ bool tile_compute(const swe_mesh_t &m, const swe_state_t &s, const Phys &p, float cfl,
                                              const TileBuf &B, const Item &it, float dt, uint32_t in_col,
                                              uint32_t com_col, float *F, uint32_t capE, uint32_t *red,
                                              uint64_t &computed, bool keep_pred, const Spread &sp,
@@ -398,7 +408,7 @@ __device__ __forceinline__ void tile_compute(const swe_mesh_t &m, const swe_stat
                                         ci[3 * kTileCells + tid], STAGE ? cc[tid] : 0.0f,
                                         STAGE ? cc[kTileCells + tid] : 0.0f, STAGE ? cc[2 * kTileCells + tid] : 0.0f,
                                         STAGE ? cc[3 * kTileCells + tid] : 0.0f, sdh, sdhu, sdhv, lam, wet, bound,
-                                        keep_pred ? B.c + 6 * kTileCells + tid : nullptr);
+                                        keep_pred ? B.c + (STAGE ? 0 : 6) * kTileCells + tid : nullptr);
     }
     if (STAGE == 1) {
         const int any_wet = __syncthreads_or(wet);
@@ -409,7 +419,9 @@ __device__ __forceinline__ void tile_compute(const swe_mesh_t &m, const swe_stat
             computed += it.cells;
         }
         if (sp.list && tid < 32u && (any_wet || s.blk[kBlkWords * b + kBlkForced] != 0u)) spread_warp(m, s, sp, b);
+        return any_wet != 0;
     }
+    return false;
 }
 
 // One stage over the current tile work items: items blockIdx.x, + gridDim.x, ...

@@ -48,6 +48,7 @@ KERNELS = {"tiled": 0, "plain": 1, "persistent": 2}
 # "auto": the persistent kernel while few blocks are active (its phases are latency-bound), the
 # 256-cell block kernel once more than this fraction of blocks is active (issue-bound work).
 AUTO_DENSE_FRACTION = 0.25
+PERSISTENT_EXTRA_TILES = 192  # kExtraCap of the persistent kernel
 
 
 def _i32(a: NDArray) -> NDArray[np.int32]:
@@ -156,10 +157,15 @@ class ResidentEngine:
     def _kernel(self) -> int:
         if self.stage_kernel == "auto":
             dense = self._active_blocks > AUTO_DENSE_FRACTION * self.n_blocks
-            return KERNELS["plain"] if dense else KERNELS["persistent"]
+            return KERNELS["plain"] if dense or not self._persistent_fits else KERNELS["persistent"]
         if self.stage_kernel not in KERNELS:
             raise ValueError(f"stage_kernel must be one of {sorted(KERNELS)} or 'auto', got {self.stage_kernel!r}")
         return KERNELS[self.stage_kernel]
+
+    @property
+    def _persistent_fits(self) -> bool:
+        """The persistent kernel gives every CTA one seat and up to PERSISTENT_EXTRA_TILES other tiles a step."""
+        return 4 * self.n_blocks <= self.grid(KERNELS["persistent"]) * (1 + PERSISTENT_EXTRA_TILES)
 
     def _alloc_state(self) -> None:
         n, nb, ni, dev = self.layout.n_padded_cells, self.n_blocks, self.n_inst, self.device
