@@ -116,20 +116,20 @@ typedef struct {
     float *h1, *hu1, *hv1, *h1_lo; /* Heun predictor */
     float *clamp_mass;             /* per-cell positivity-clamp volume (diagnostic) */
     uint32_t *blk;                 /* 3 words per block: wet, active, forced */
-    uint32_t *active_list;         /* 2 x n_blocks: active blocks of the current step (first half; the
-                                      persistent kernel alternates halves within a launch) */
+    uint32_t *active_list;         /* 2 x n_blocks: active blocks of the current step (first half) */
     uint32_t *items;               /* 2 x 4 words per 64-cell tile: work items of the tiled kernels (first
-                                      half; the persistent kernel alternates halves within a launch) */
+                                      half); the persistent kernel queues tile ids in the second half */
     uint32_t *sched;               /* 16 words: [0] active blocks, [1] next blocks, [2] done CTAs, [3] work items,
-                                      [4] next items, [6..7] uint64 cells computed over real steps,
-                                      [10] step epoch and [11] previous active blocks (persistent kernel),
-                                      others zero */
+                                      [4] next items, [6..7] uint64 cells computed over real steps; the
+                                      persistent kernel's [10] step epoch, [11] start-list tiles taken and
+                                      [12..15] its two tile queues' lengths and taken counts; others zero */
     uint32_t *dt_buf;              /* 4 words per instance: [0] this step's dt (float bits, 0 = no-op),
                                       [1] the next step's CFL bound */
     swe_ctrl_t *ctrl;              /* one per instance */
     uint32_t *sync;                /* 64 zeroed words: the grid barrier of the persistent kernel (kernel 2) */
-    uint32_t *marks;               /* 2 words per block, zeroed with sched word 10 at the start of a run: the
-                                      epochs at which a block was listed and its two-ring spread (kernel 2) */
+    uint32_t *marks;               /* 2 words per block, zeroed with sched word 10 at the start of a run: word
+                                      0 the epoch of the latest step the block is active in (kernel 2), word
+                                      1 unused */
     float *open_vol;               /* 4 words per open edge, zeroed at the start of a run: the volume that
                                       left (hi, lo) and entered (hi, lo) the mesh through it, as exact
                                       float pairs (the per-edge form of TALLY_RESIDENT_GLSL,

@@ -220,7 +220,7 @@ __device__ bool seat_predictor(const swe_mesh_t &m, const swe_state_t &s, const 
         }
         tile_compute<0, COMP, CLAMP, kPersistThreads, OPEN>(m, s, p, cfl, B0, unpack(ss.seat_item),
                                                             __uint_as_float(ss.seat_dt), 0u, 6u, F, L.capE, sh.red,
-                                                            computed, true, Spread{});
+                                                            computed, true);
         fence_proxy_async();
         __syncthreads();
     }
@@ -257,7 +257,7 @@ __device__ bool seat_predictor(const swe_mesh_t &m, const swe_state_t &s, const 
             if (!seat_wait(s, B0, ph, 0u)) return false;
             tile_compute<0, COMP, CLAMP, kPersistThreads, OPEN>(m, s, p, cfl, B0, unpack(ss.seat_item),
                                                                 __uint_as_float(ss.seat_dt), 0u, 6u, F, L.capE, sh.red,
-                                                                computed, true, Spread{});
+                                                                computed, true);
         } else {
             if (tid == 0) {
                 ss.extra[ss.n_extra] = ss.take_item;
@@ -268,7 +268,7 @@ __device__ bool seat_predictor(const swe_mesh_t &m, const swe_state_t &s, const 
             if (!seat_wait(s, B1, ph, 1u)) return false;
             tile_compute<0, COMP, CLAMP, kPersistThreads, OPEN>(m, s, p, cfl, B1, unpack(ss.take_item),
                                                                 __uint_as_float(ss.take_dt), 0u, 6u, F, L.capE, sh.red,
-                                                                computed, false, Spread{});
+                                                                computed, false);
         }
         fence_proxy_async();
         __syncthreads();
@@ -291,7 +291,7 @@ __device__ bool seat_corrector(const swe_mesh_t &m, const swe_state_t &s, const 
     if (ss.seat_active) {
         const Item it = unpack(ss.seat_item);
         const bool wet = tile_compute<1, COMP, CLAMP, kPersistThreads, OPEN>(
-            m, s, p, cfl, B0, it, __uint_as_float(ss.seat_dt), 6u, 0u, F, L.capE, sh.red, computed, true, Spread{});
+            m, s, p, cfl, B0, it, __uint_as_float(ss.seat_dt), 6u, 0u, F, L.capE, sh.red, computed, true);
         if (!all_active && tid < 32u && (wet || ss.seat_forced != 0u))
             mark_ring(m, s, it.tile >> 2, epoch, next, qpar, ss.ring_n <= kRingCache ? ss.ring : nullptr, ss.ring_n);
         fence_proxy_async();
@@ -303,8 +303,7 @@ __device__ bool seat_corrector(const swe_mesh_t &m, const swe_state_t &s, const 
         if (!seat_wait(s, B1, ph, 1u)) return false;
         const Item it = unpack(ss.extra[w]);
         const bool wet = tile_compute<1, COMP, CLAMP, kPersistThreads, OPEN>(
-            m, s, p, cfl, B1, it, __uint_as_float(ss.extra_dt[w]), 0u, 6u, F, L.capE, sh.red, computed, false,
-            Spread{});
+            m, s, p, cfl, B1, it, __uint_as_float(ss.extra_dt[w]), 0u, 6u, F, L.capE, sh.red, computed, false);
         if (!all_active && tid < 32u && (wet || s.blk[kBlkWords * (it.tile >> 2) + kBlkForced] != 0u))
             mark_ring(m, s, it.tile >> 2, epoch, next, qpar, nullptr, 0u);
         fence_proxy_async();

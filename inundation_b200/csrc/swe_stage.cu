@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(kTileThreads, 8)
     __syncthreads();
     uint32_t k = 0;
     uint64_t computed = 0;
-    if (!tiled_pass<STAGE, COMP, CLAMP, kTileThreads, false, OPEN>(m, s, p, cfl, smem, sh, k, computed, Spread{}, sums))
+    if (!tiled_pass<STAGE, COMP, CLAMP, kTileThreads, OPEN>(m, s, p, cfl, smem, sh, k, computed, sums))
         return;
     if (STAGE == 1 && threadIdx.x == 0 && computed)
         atomicAdd(reinterpret_cast<unsigned long long *>(s.sched + kSchedComputed), computed);

@@ -236,67 +236,8 @@ struct TiledShared {
     uint32_t count;
 };
 
-// Where the persistent kernel builds the next step's work lists: the next half
-// of the block list and the work items, and this step's epoch (the marks of
-// blocks listed, or spread, in this step hold it). list == nullptr: no spreading.
-struct Spread {
-    uint32_t *list;
-    uint4 *items;
-    uint32_t epoch;
-};
-
-// Append block b and its tiles to the next lists (one lane).
-__device__ __forceinline__ void list_block(const swe_mesh_t &m, const swe_state_t &s, const Spread &sp, uint32_t b) {
-    const uint32_t cells = m.block_cells[b];
-    const uint32_t n_items = (cells + kTileCells - 1) / kTileCells;
-    const uint32_t pos = atomicAdd(&s.sched[kSchedNext], 1u);
-    const uint32_t ipos = atomicAdd(&s.sched[kSchedNextItems], n_items);
-    if (pos < m.n_blocks) sp.list[pos] = b;
-    const uint32_t inst = m.block_inst[b];
-    for (uint32_t q = 0; q < n_items && ipos + q < 4u * m.n_blocks; ++q) {
-        const uint32_t t = 4u * b + q;
-        const uint32_t l0 = m.sub_lcsr_ptr[t];
-        sp.items[ipos + q] = make_item(t, min(static_cast<uint32_t>(kTileCells), cells - q * kTileCells), m.sub_ptr[t],
-                                       l0, m.sub_count[t], m.sub_lcsr_ptr[t + 1] - l0, inst);
-    }
-}
-
-// The dilation, spread from a wet (or forced) block: block b and every block of
-// its two-ring are active next step. The two-ring relation is symmetric, so
-// spreading from every wet block lists exactly the blocks whose two-ring holds
-// a wet block, as the gather over each block's two-ring does
-// (resident.py:778-805). Each block is spread once per step and listed once
-// (the marks' epochs). One warp.
-__device__ __forceinline__ void spread_warp(const swe_mesh_t &m, const swe_state_t &s, const Spread &sp, uint32_t b) {
-    const uint32_t lane = threadIdx.x & 31u;
-    uint32_t fresh = 0u;
-    if (lane == 0) fresh = atomicExch(&s.marks[2u * b + 1u], sp.epoch) != sp.epoch;
-    if (!__shfl_sync(0xFFFFFFFFu, fresh, 0)) return;
-    const uint32_t k0 = m.ring_ptr[b], total = m.ring_ptr[b + 1] - k0 + 1u;
-    for (uint32_t base = 0; base < total; base += 32u) {
-        const uint32_t idx = base + lane;
-        bool listed = false;
-        uint32_t nb = 0u;
-        if (idx < total) {
-            nb = idx == 0u ? b : m.ring_idx[k0 + idx - 1u];
-            listed = atomicExch(&s.marks[2u * nb], sp.epoch) != sp.epoch;
-        }
-        if (listed) list_block(m, s, sp, nb);
-    }
-}
-
-// The same from one thread (sources).
-__device__ __forceinline__ void spread_thread(const swe_mesh_t &m, const swe_state_t &s, const Spread &sp, uint32_t b) {
-    if (s.marks[2u * b + 1u] == sp.epoch || atomicExch(&s.marks[2u * b + 1u], sp.epoch) == sp.epoch) return;
-    const uint32_t k0 = m.ring_ptr[b], k1 = m.ring_ptr[b + 1];
-    if (atomicExch(&s.marks[2u * b], sp.epoch) != sp.epoch) list_block(m, s, sp, b);
-    for (uint32_t k = k0; k < k1; ++k) {
-        const uint32_t nb = m.ring_idx[k];
-        if (atomicExch(&s.marks[2u * nb], sp.epoch) != sp.epoch) list_block(m, s, sp, nb);
-    }
-}
-
-// Shared-memory bytes of a tile pass: two staged buffers, and with KEEP the
+// Shared-memory bytes of a tile pass: two staged buffers, and with `keep` (the
+// persistent kernel, whose buffers keep their records from step to step) the
 // flux words in arrays of their own (7 per record).
 __host__ __device__ inline size_t tiled_smem_bytes(uint32_t max_edges, uint32_t max_slots, bool keep) {
     const TilePlan L = tile_plan(max_edges, max_slots, 10u);
@@ -314,8 +255,7 @@ template <int STAGE, bool COMP, bool CLAMP, int TPB, bool OPEN>
 __device__ __forceinline__ bool tile_compute(const swe_mesh_t &m, const swe_state_t &s, const Phys &p, float cfl,
                                              const TileBuf &B, const Item &it, float dt, uint32_t in_col,
                                              uint32_t com_col, float *F, uint32_t capE, uint32_t *red,
-                                             uint64_t &computed, bool keep_pred, const Spread &sp,
-                                             float *sums = nullptr) {
+                                             uint64_t &computed, bool keep_pred, float *sums = nullptr) {
     const uint32_t tid = threadIdx.x;
     const uint32_t b = it.tile >> 2;
     if (STAGE == 0 && (it.tile & 3u) == 0u && tid == 0) s.blk[kBlkWords * b + kBlkWet] = 0u;
@@ -418,7 +358,6 @@ __device__ __forceinline__ bool tile_compute(const swe_mesh_t &m, const swe_stat
             if (bmin != kNoBound) atomicMin(&s.dt_buf[kDtWords * it.inst + 1], bmin);
             computed += it.cells;
         }
-        if (sp.list && tid < 32u && (any_wet || s.blk[kBlkWords * b + kBlkForced] != 0u)) spread_warp(m, s, sp, b);
         return any_wet != 0;
     }
     return false;
@@ -428,37 +367,18 @@ __device__ __forceinline__ bool tile_compute(const swe_mesh_t &m, const swe_stat
 // `smem` holds the two mbarriers (initialised by the caller) and the two staged
 // buffers; `k` counts this CTA's buffer uses across calls (their mbarrier
 // phases); computed cells of the corrector accumulate in `computed`.
-// KEEP (the persistent kernel, which runs the corrector right after the
-// predictor over the same list): one buffer layout for both stages, flux words
-// in arrays of their own, and the predictor's new state kept in columns 6..9;
-// when every CTA has at most one item, the corrector then computes from the
-// predictor's staged tile without staging anything.
 // Returns false when staged data did not arrive within the wait bound (the
 // copies in flight have had one more bounded wait; the caller must stop).
-template <int STAGE, bool COMP, bool CLAMP, int TPB, bool KEEP, bool OPEN>
+template <int STAGE, bool COMP, bool CLAMP, int TPB, bool OPEN>
 __device__ bool tiled_pass(const swe_mesh_t &m, const swe_state_t &s, const Phys &p, float cfl, unsigned char *smem,
-                           TiledShared<TPB> &sh, uint32_t &k, uint64_t &computed, const Spread &sp = Spread{},
-                           float *sums = nullptr) {
-    constexpr uint32_t nc = (STAGE || KEEP) ? 10u : 6u;
+                           TiledShared<TPB> &sh, uint32_t &k, uint64_t &computed, float *sums = nullptr) {
+    constexpr uint32_t nc = STAGE ? 10u : 6u;
     const TilePlan L = tile_plan(m.max_sub_edges, m.max_sub_slots, nc);
-    float *F = KEEP ? reinterpret_cast<float *>(smem + L.total) : nullptr;
     uint32_t *red = sh.red;
     uint4 *items = sh.items;
     uint32_t *dts = sh.dts;
     const uint4 *work = reinterpret_cast<const uint4 *>(s.items);
     const uint32_t tid = threadIdx.x;
-
-    if (KEEP && STAGE == 1 && sh.count <= gridDim.x) {
-        // The predictor's tile of this CTA is still staged (same list, one item per CTA).
-        if (blockIdx.x >= sh.count) return true;
-        const uint32_t kb = (k - 1u) & 1u;
-        const uint32_t dt_bits = dts[kb];
-        if (dt_bits != 0u)
-            tile_compute<1, COMP, CLAMP, TPB, OPEN>(m, s, p, cfl, tile_buf(smem, L, kb), unpack(items[kb]),
-                                              __uint_as_float(dt_bits), 6u, 0u, F, L.capE, red, computed, false, sp, sums);
-        __syncthreads();
-        return true;
-    }
 
     if (tid < 32u) {
         // The item count and this CTA's first item in one round trip (the item buffer
@@ -487,7 +407,6 @@ __device__ bool tiled_pass(const swe_mesh_t &m, const swe_state_t &s, const Phys
     __syncthreads();
     const uint32_t count = sh.count;
     if (blockIdx.x >= count) return true;
-    const bool keep_pred = KEEP && STAGE == 0 && count <= gridDim.x;
 
     for (uint32_t w = blockIdx.x; w < count; w += gridDim.x, ++k) {
         const TileBuf B = tile_buf(smem, L, k & 1u);
@@ -513,7 +432,7 @@ __device__ bool tiled_pass(const swe_mesh_t &m, const swe_state_t &s, const Phys
         const uint32_t dt_bits = dts[k & 1u];
         if (dt_bits != 0u)
             tile_compute<STAGE, COMP, CLAMP, TPB, OPEN>(m, s, p, cfl, B, unpack(items[k & 1u]), __uint_as_float(dt_bits), 0u,
-                                                  6u, F, L.capE, red, computed, keep_pred, sp, sums);
+                                                  6u, nullptr, L.capE, red, computed, false, sums);
         // This buffer is refilled by bulk copies two items on.
         fence_proxy_async();
         __syncthreads();
