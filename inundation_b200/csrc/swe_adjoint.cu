@@ -77,14 +77,16 @@ __device__ __forceinline__ CellFwd cell_forward(const Phys &p, float dt, float A
     c.drag = film_drag(p, c.h_new, dt);
     c.hu_b = c.hu_a * c.drag;
     c.hv_b = c.hv_a * c.drag;
-    c.u = c.hu_b / c.h_new;
-    c.v = c.hv_b / c.h_new;
+    const float inv_h = 1.0f / c.h_new;
+    c.u = c.hu_b * inv_h;
+    c.v = c.hv_b * inv_h;
     c.spd = sqrtf(c.u * c.u + c.v * c.v);
     c.P = pow43(c.h_new);
     c.Sf = p.g * n * n * c.spd / c.P;
     c.den = 1.0f + dt * c.Sf;
-    c.hu_new = c.hu_b / c.den;
-    c.hv_new = c.hv_b / c.den;
+    const float inv_den = 1.0f / c.den;
+    c.hu_new = c.hu_b * inv_den;
+    c.hv_new = c.hv_b * inv_den;
     return c;
 }
 
@@ -163,15 +165,17 @@ __device__ EdgeGrad edge_words_rev(const Phys &p, bool wall, float nx, float ny,
     // ---- primal (face_states, hllc_speeds_fast, hllc) ----
     const float hLs = gmax(0.0f, hL - dzL);
     const float hRs = gmax(0.0f, hR - dzR);
-    const float uL = safe_vel(p, hL, huL), vL = safe_vel(p, hL, hvL);
-    const float uR = safe_vel(p, hR, huR), vR = safe_vel(p, hR, hvR);
+    float uL, vL, uR, vR;
+    safe_vel2(p, hL, huL, hvL, uL, vL);
+    safe_vel2(p, hR, huR, hvR, uR, vR);
     const float huLs = hLs * uL, hvLs = hLs * vL, huRs = hRs * uR, hvRs = hRs * vR;
     const float hqnL = huLs * nx + hvLs * ny;
     const float hqtL = -huLs * ny + hvLs * nx;
     const float hqnR = huRs * nx + hvRs * ny;
     const float hqtR = -huRs * ny + hvRs * nx;
-    const float unL = safe_vel(p, hLs, hqnL), utL = safe_vel(p, hLs, hqtL);
-    const float unR = safe_vel(p, hRs, hqnR), utR = safe_vel(p, hRs, hqtR);
+    float unL, utL, unR, utR;
+    safe_vel2(p, hLs, hqnL, hqtL, unL, utL);
+    safe_vel2(p, hRs, hqnR, hqtR, unR, utR);
     const float cL = sqrtf(p.g * gmax(hLs, 0.0f));
     const float cR = sqrtf(p.g * gmax(hRs, 0.0f));
     const float sqL = sqrtf(gmax(hLs, 0.0f));

@@ -23,13 +23,19 @@ __device__ __forceinline__ float gmin(float x, float y) { return (y < x) ? y : x
 __device__ __forceinline__ float gmax(float x, float y) { return (x < y) ? y : x; }
 __device__ __forceinline__ float gclamp(float x, float lo, float hi) { return gmin(gmax(x, lo), hi); }
 
-// x^(4/3) for x > 0: cube root by Newton's iteration r <- (2r + x/r^2)/3
+// Divisions: GLSL divides to within 2.5 ulp, so a product by a correctly
+// rounded reciprocal (or by the float 1/3) is a quotient the reference admits.
+// Quotients that share a denominator use one reciprocal; host and device
+// evaluate the same expressions.
+constexpr float kOneThird = 1.0f / 3.0f;
+
+// x^(4/3) for x > 0: cube root by Newton's iteration r <- (2r + x/r^2) * (1/3)
 // from the exponent-thirds estimate bits(x)/3 + (2/3)*127*2^23, then x*r.
 // Basic IEEE operations only, so host and device agree exactly.
 __device__ __forceinline__ float pow43(float x) {
     float r = __uint_as_float(__float_as_uint(x) / 3u + 0x2A555555u);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) r = (2.0f * r + x / (r * r)) / 3.0f;
+    for (int k = 0; k < 4; ++k) r = (2.0f * r + x / (r * r)) * kOneThird;
     return x * r;
 }
 
@@ -37,6 +43,19 @@ __device__ __forceinline__ float pow43(float x) {
 __device__ __forceinline__ float safe_vel(const Phys &p, float h, float hq) {
     const float e = kFilmDepths * p.dry_tol;
     return (h > p.dry_tol) ? 2.0f * h * hq / (h * h + gmax(h * h, e * e)) : 0.0f;
+}
+
+// safe_vel of two momenta of one depth, with one reciprocal of their denominator.
+__device__ __forceinline__ void safe_vel2(const Phys &p, float h, float hq1, float hq2, float &v1, float &v2) {
+    if (h > p.dry_tol) {
+        const float e = kFilmDepths * p.dry_tol;
+        const float inv = 1.0f / (h * h + gmax(h * h, e * e));
+        v1 = 2.0f * h * hq1 * inv;
+        v2 = 2.0f * h * hq2 * inv;
+    } else {
+        v1 = 0.0f;
+        v2 = 0.0f;
+    }
 }
 
 // HLLC wave-speed bounds: Roe average, blended continuously into Toro's
@@ -94,8 +113,9 @@ __device__ __forceinline__ void hllc_speeds_fast(const Phys &p, float hL, float 
 // HLLC flux in the face frame (Toro 2001); smax is the largest speed assumed.
 __device__ __forceinline__ void hllc(const Phys &p, float hL, float hqnL, float hqtL, float hR, float hqnR,
                                      float hqtR, float &Fh, float &Fhn, float &Fht, float &smax) {
-    const float unL = safe_vel(p, hL, hqnL), utL = safe_vel(p, hL, hqtL);
-    const float unR = safe_vel(p, hR, hqnR), utR = safe_vel(p, hR, hqtR);
+    float unL, utL, unR, utR;
+    safe_vel2(p, hL, hqnL, hqtL, unL, utL);
+    safe_vel2(p, hR, hqnR, hqtR, unR, utR);
     float SL, SR;
     hllc_speeds_fast(p, hL, unL, hR, unR, SL, SR);
     smax = gmax(fabsf(SL), fabsf(SR));
@@ -132,8 +152,9 @@ __device__ __forceinline__ void face_states(const Phys &p, float hL, float huL, 
                                             float &hqnL, float &hqtL, float &hRs, float &hqnR, float &hqtR) {
     hLs = gmax(0.0f, hL - dzL);
     hRs = gmax(0.0f, hR - dzR);
-    const float uL = safe_vel(p, hL, huL), vL = safe_vel(p, hL, hvL);
-    const float uR = safe_vel(p, hR, huR), vR = safe_vel(p, hR, hvR);
+    float uL, vL, uR, vR;
+    safe_vel2(p, hL, huL, hvL, uL, vL);
+    safe_vel2(p, hR, huR, hvR, uR, vR);
     const float huLs = hLs * uL, hvLs = hLs * vL, huRs = hRs * uR, hvRs = hRs * vR;
     hqnL = huLs * nx + hvLs * ny;
     hqtL = -huLs * ny + hvLs * nx;

@@ -43,12 +43,13 @@ __device__ __forceinline__ void update_cell(const swe_state_t &s, const Phys &p,
         const float drag = film_drag(p, h_new, dt);
         hu_new *= drag;
         hv_new *= drag;
-        const float u_ = hu_new / h_new, v_ = hv_new / h_new;
+        const float inv_h = 1.0f / h_new;
+        const float u_ = hu_new * inv_h, v_ = hv_new * inv_h;
         const float spd = sqrtf(u_ * u_ + v_ * v_);
         const float Sf = p.g * n * n * spd / pow43(h_new);
-        const float den = 1.0f + dt * Sf;
-        hu_new = hu_new / den;
-        hv_new = hv_new / den;
+        const float inv_den = 1.0f / (1.0f + dt * Sf);
+        hu_new = hu_new * inv_den;
+        hv_new = hv_new * inv_den;
     }
     if (STAGE == 0) {
         s.h1[i] = h_new;

@@ -99,19 +99,38 @@ static inline float gmin(float x, float y) { return (y < x) ? y : x; }
 static inline float gmax(float x, float y) { return (x < y) ? y : x; }
 static inline float gclamp(float x, float lo, float hi) { return gmin(gmax(x, lo), hi); }
 
-/* x^(1/3) for x > 0 by Newton's iteration r <- (2r + x/r^2)/3 from the
+/* Divisions: GLSL divides to within 2.5 ulp, so a product by a correctly
+   rounded reciprocal (or by the float 1/3) is a quotient the reference
+   admits. Quotients that share a denominator use one reciprocal, in the
+   same expressions as the CUDA kernels. */
+static const float ONE_THIRD = 1.0f / 3.0f;
+
+/* x^(1/3) for x > 0 by Newton's iteration r <- (2r + x/r^2) * (1/3) from the
    bit-level estimate bits(x)/3 + (2/3)*127*2^23 (the exponent divided by
    three), then x * r. Basic IEEE operations only. */
 static float pow43(float x) {
     uint32_t i = fbits(x);
     float r = bitsf(i / 3u + 0x2A555555u);
-    for (int k = 0; k < 4; ++k) r = (2.0f * r + x / (r * r)) / 3.0f;
+    for (int k = 0; k < 4; ++k) r = (2.0f * r + x / (r * r)) * ONE_THIRD;
     return x * r;
 }
 
 static float safe_vel(const oracle_t *o, float h_, float hq) {
     float e_ = FILM_DEPTHS * o->dry_tol;
     return (h_ > o->dry_tol) ? 2.0f * h_ * hq / (h_ * h_ + gmax(h_ * h_, e_ * e_)) : 0.0f;
+}
+
+/* safe_vel of two momenta of one depth, with one reciprocal of their denominator. */
+static void safe_vel2(const oracle_t *o, float h_, float hq1, float hq2, float *v1, float *v2) {
+    if (h_ > o->dry_tol) {
+        float e_ = FILM_DEPTHS * o->dry_tol;
+        float inv = 1.0f / (h_ * h_ + gmax(h_ * h_, e_ * e_));
+        *v1 = 2.0f * h_ * hq1 * inv;
+        *v2 = 2.0f * h_ * hq2 * inv;
+    } else {
+        *v1 = 0.0f;
+        *v2 = 0.0f;
+    }
 }
 
 static void hllc_speeds(const oracle_t *o, float hL, float unL, float hR, float unR, float *SLo, float *SRo) {
@@ -137,8 +156,9 @@ static void hllc_speeds(const oracle_t *o, float hL, float unL, float hR, float 
 static void hllc(const oracle_t *o, float hL, float hqnL, float hqtL, float hR, float hqnR, float hqtR,
                  float *Fh, float *Fhn, float *Fht, float *Smax) {
     float g = o->g;
-    float unL = safe_vel(o, hL, hqnL), utL = safe_vel(o, hL, hqtL);
-    float unR = safe_vel(o, hR, hqnR), utR = safe_vel(o, hR, hqtR);
+    float unL, utL, unR, utR;
+    safe_vel2(o, hL, hqnL, hqtL, &unL, &utL);
+    safe_vel2(o, hR, hqnR, hqtR, &unR, &utR);
     float SL, SR;
     hllc_speeds(o, hL, unL, hR, unR, &SL, &SR);
     *Smax = gmax(fabsf(SL), fabsf(SR));
@@ -171,8 +191,9 @@ static void face_states(const oracle_t *o, float hL, float huL, float hvL, float
                         float *hRs, float *hqnR, float *hqtR) {
     *hLs = gmax(0.0f, hL - dzL);
     *hRs = gmax(0.0f, hR - dzR);
-    float uL = safe_vel(o, hL, huL), vL = safe_vel(o, hL, hvL);
-    float uR = safe_vel(o, hR, huR), vR = safe_vel(o, hR, hvR);
+    float uL, vL, uR, vR;
+    safe_vel2(o, hL, huL, hvL, &uL, &vL);
+    safe_vel2(o, hR, huR, hvR, &uR, &vR);
     float huLs = *hLs * uL, hvLs = *hLs * vL, huRs = *hRs * uR, hvRs = *hRs * vR;
     *hqnL = huLs * nx_ + hvLs * ny_;
     *hqtL = -huLs * ny_ + hvLs * nx_;
@@ -443,13 +464,14 @@ void oracle_update_stage(oracle_t *o, int stage, int compensated, int track_clam
         }
         if (h_new >= o->dry_tol) {
             float n = o->n_mann[i];
-            float u_ = hu_new / h_new, v_ = hv_new / h_new;
+            float inv_h = 1.0f / h_new;
+            float u_ = hu_new * inv_h, v_ = hv_new * inv_h;
             float spd = sqrtf(u_ * u_ + v_ * v_);
             float h43 = pow43(h_new);
             float Sf = o->g * n * n * spd / h43;
-            float den = 1.0f + dt * Sf;
-            hu_new = hu_new / den;
-            hv_new = hv_new / den;
+            float inv_den = 1.0f / (1.0f + dt * Sf);
+            hu_new = hu_new * inv_den;
+            hv_new = hv_new * inv_den;
         }
         float hf = 0.0f;
         if (compensated) {
