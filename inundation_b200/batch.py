@@ -251,6 +251,8 @@ def autotune(
     state, timed with CUDA events on the solver's stream (best of
     ``rounds``); the fastest is set on the solver. The state is reset to the
     initial state afterwards. Results are remembered per layout signature.
+    Persistent candidates whose grid cannot hold every tile of a step are
+    skipped.
     """
     key = _signature(solver)
     if key in _TUNED:
@@ -263,6 +265,8 @@ def autotune(
     results = []
     for kernel, per_sm in candidates:
         solver.stage_kernel, solver.ctas_per_sm = kernel, per_sm
+        if kernel == "persistent" and not solver._persistent_fits:
+            continue  # its grid cannot hold every tile of a step
         solver.steps_per_graph = steps
         best_ms = math.inf
         for _ in range(rounds):

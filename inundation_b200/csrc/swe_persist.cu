@@ -44,7 +44,7 @@ namespace swe {
 // CTA that finds a tile of its seat or of the queue inactive clears it. At the
 // end of a launch one pass turns the last marks into the flags, block list and
 // tile work items the other kernels and the host read.
-constexpr uint32_t kExtraCap = 192;  // tiles a CTA computes besides its seat in one step
+constexpr uint32_t kExtraCap = 512;  // tiles a CTA computes besides its seat in one step
 constexpr uint32_t kRingCache = 96;  // blocks of the seat's two-ring kept in shared memory
 constexpr uint32_t kNoTile = 0xFFFFFFFFu;
 

@@ -48,7 +48,7 @@ KERNELS = {"tiled": 0, "plain": 1, "persistent": 2}
 # "auto": the persistent kernel while few blocks are active (its phases are latency-bound), the
 # 256-cell block kernel once more than this fraction of blocks is active (issue-bound work).
 AUTO_DENSE_FRACTION = 0.25
-PERSISTENT_EXTRA_TILES = 192  # kExtraCap of the persistent kernel
+PERSISTENT_EXTRA_TILES = 512  # kExtraCap of the persistent kernel
 
 
 def _i32(a: NDArray) -> NDArray[np.int32]:
