@@ -61,6 +61,7 @@ struct SeatShared {
     uint32_t seat_forced;
     uint32_t ring_n;
     uint32_t ring[kRingCache];
+    uint32_t ring_active[kRingCache / 32];  // ring blocks active in this step (seat only)
     uint32_t qlen;            // tiles queued for this step
     uint32_t take;            // a taken tile (kNoTile: the queue is empty)
     uint4 take_item;
@@ -83,15 +84,21 @@ __device__ __forceinline__ uint32_t *tile_queue(const swe_mesh_t &m, const swe_s
 // Mark block b and its two-ring active for the step of epoch `next` (one warp);
 // a block whose old mark is neither `next` nor `cur` (not active now) becomes
 // active: its tiles join the next step's queue (parity qpar). ring: the cached
-// two-ring, or nullptr to read it from global memory.
+// two-ring, or nullptr to read it from global memory; active: bits of ring
+// blocks known to be active now (and block b is), which need no exchange.
 __device__ __forceinline__ void mark_ring(const swe_mesh_t &m, const swe_state_t &s, uint32_t b, uint32_t cur,
-                                          uint32_t next, uint32_t qpar, const uint32_t *ring, uint32_t ring_n) {
+                                          uint32_t next, uint32_t qpar, const uint32_t *ring, uint32_t ring_n,
+                                          const uint32_t *active = nullptr) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t k0 = ring ? 0u : m.ring_ptr[b];
     const uint32_t n = ring ? ring_n : m.ring_ptr[b + 1] - k0;
     uint32_t *q = tile_queue(m, s, qpar);
     for (uint32_t k = lane; k <= n; k += 32u) {
         const uint32_t nb = k == 0u ? b : (ring ? ring[k - 1u] : m.ring_idx[k0 + k - 1u]);
+        if (active && (k == 0u || ((active[(k - 1u) >> 5] >> ((k - 1u) & 31u)) & 1u))) {
+            s.marks[2u * nb] = next;  // active now: no tiles to queue
+            continue;
+        }
         const uint32_t old = atomicExch(&s.marks[2u * nb], next);
         if (old != next && old != cur) {
             const uint32_t n_tiles = (m.block_cells[nb] + kTileCells - 1u) / kTileCells;
@@ -191,7 +198,35 @@ __device__ bool seat_predictor(const swe_mesh_t &m, const swe_state_t &s, const 
     float *F = reinterpret_cast<float *>(smem + L.total);
     const TileBuf B0 = tile_buf(smem, L, 0u), B1 = tile_buf(smem, L, 1u);
     const uint32_t tid = threadIdx.x;
-    if (tid == 0) {
+    if (!OPEN && ss.seat != kNoTile) {
+        // The seat's predictor starts before its activity and dt are known: both arrive
+        // while its fluxes are computed (the update of an inactive seat keeps nothing
+        // anyone reads). An open mesh's tallies need dt in the flux loop: no early start.
+        const Item it = unpack(ss.seat_item);
+        const uint32_t b = ss.seat >> 2;
+        if (!ss.state_ok || sources) {
+            if (tid < 32u) seat_issue<0>(m, s, ss.seat_item, B0, true);
+            if (!seat_wait(s, B0, ph, 0u)) return false;
+        }
+        const LateDt late{s.dt_buf + kDtWords * it.inst, s.marks + 2u * b, epoch, all_active ? 1u : 0u, sh.late};
+        tile_compute<0, COMP, CLAMP, kPersistThreads, OPEN>(m, s, p, cfl, B0, it, 0.0f, 0u, 6u, F, L.capE, sh.red,
+                                                            computed, true, nullptr, &late);
+        fence_proxy_async();
+        if (tid == 0) {
+            ss.n_extra = 0u;
+            ss.qlen = step == 0u ? *reinterpret_cast<volatile uint32_t *>(s.sched + kSchedItems)
+                                 : *reinterpret_cast<volatile uint32_t *>(s.sched + kSchedQProd + (step & 1u));
+            const uint32_t dt = sh.late[1];
+            ss.seat_active = sh.late[0] != 0u ? 1u : 0u;
+            ss.seat_dt = sh.late[0];
+            if (dt != 0u && !ss.seat_active) {
+                if ((ss.seat & 3u) == 0u) s.blk[kBlkWords * b + kBlkActive] = 0u;
+                ss.seat = kNoTile;  // free for a queued tile; the records stay staged
+                ss.state_ok = 0u;   // another CTA may compute the tile before it returns here
+            }
+        }
+        __syncthreads();
+    } else if (tid == 0) {
         ss.n_extra = 0u;
         ss.qlen = step == 0u ? *reinterpret_cast<volatile uint32_t *>(s.sched + kSchedItems)
                              : *reinterpret_cast<volatile uint32_t *>(s.sched + kSchedQProd + (step & 1u));
@@ -213,7 +248,7 @@ __device__ bool seat_predictor(const swe_mesh_t &m, const swe_state_t &s, const 
         }
     }
     __syncthreads();
-    if (ss.seat_active) {
+    if (OPEN && ss.seat_active) {
         if (!ss.state_ok || sources) {
             if (tid < 32u) seat_issue<0>(m, s, ss.seat_item, B0, true);
             if (!seat_wait(s, B0, ph, 0u)) return false;
@@ -223,6 +258,16 @@ __device__ bool seat_predictor(const swe_mesh_t &m, const swe_state_t &s, const 
                                                             computed, true);
         fence_proxy_async();
         __syncthreads();
+    }
+    if (!OPEN && !all_active && ss.seat_active && ss.ring_n <= kRingCache && tid >= 32u && tid < 64u) {
+        // which blocks of the seat's two-ring are active now (read beside the first take)
+        const uint32_t lane = tid & 31u;
+        for (uint32_t w = 0; w * 32u < ss.ring_n; ++w) {
+            const uint32_t k = w * 32u + lane;
+            const bool act = k < ss.ring_n && s.marks[2u * ss.ring[k]] == epoch;
+            const uint32_t bits = __ballot_sync(0xFFFFFFFFu, act);
+            if (lane == 0) ss.ring_active[w] = bits;
+        }
     }
     for (;;) {
         if (ss.seat != kNoTile && ss.n_extra >= kExtraCap) break;
@@ -292,8 +337,11 @@ __device__ bool seat_corrector(const swe_mesh_t &m, const swe_state_t &s, const 
         const Item it = unpack(ss.seat_item);
         const bool wet = tile_compute<1, COMP, CLAMP, kPersistThreads, OPEN>(
             m, s, p, cfl, B0, it, __uint_as_float(ss.seat_dt), 6u, 0u, F, L.capE, sh.red, computed, true);
-        if (!all_active && tid < 32u && (wet || ss.seat_forced != 0u))
-            mark_ring(m, s, it.tile >> 2, epoch, next, qpar, ss.ring_n <= kRingCache ? ss.ring : nullptr, ss.ring_n);
+        if (!all_active && tid < 32u && (wet || ss.seat_forced != 0u)) {
+            const bool cached = ss.ring_n <= kRingCache;
+            mark_ring(m, s, it.tile >> 2, epoch, next, qpar, cached ? ss.ring : nullptr, ss.ring_n,
+                      !OPEN && cached ? ss.ring_active : nullptr);
+        }
         fence_proxy_async();
         __syncthreads();
     }

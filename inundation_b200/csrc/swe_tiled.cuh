@@ -231,10 +231,24 @@ __device__ __forceinline__ void tile_issue(const swe_mesh_t &m, const swe_state_
 // Shared words of a tile pass besides the staged buffers.
 template <int TPB>
 struct TiledShared {
+    uint32_t late[2];  // LateDt's slot
     uint32_t red[TPB / 32];
     uint4 items[2];
     uint32_t dts[2];
     uint32_t count;
+};
+
+// A predictor started before its dt and the tile's activity are known (the
+// persistent kernel's seat): thread 0 loads both at the start, and after the
+// fluxes, which need neither, publishes in slot[0] the dt the update uses (0
+// when the tile turns out inactive: the update then keeps nothing anyone reads)
+// and in slot[1] the instance's dt.
+struct LateDt {
+    const uint32_t *dt;    // the instance's dt word
+    const uint32_t *mark;  // the block's epoch word
+    uint32_t epoch;        // the epoch of an active block
+    uint32_t all;          // every block is active
+    uint32_t *slot;        // two shared words
 };
 
 // Shared-memory bytes of a tile pass: two staged buffers, and with `keep` (the
@@ -256,10 +270,16 @@ template <int STAGE, bool COMP, bool CLAMP, int TPB, bool OPEN>
 __device__ __forceinline__ bool tile_compute(const swe_mesh_t &m, const swe_state_t &s, const Phys &p, float cfl,
                                              const TileBuf &B, const Item &it, float dt, uint32_t in_col,
                                              uint32_t com_col, float *F, uint32_t capE, uint32_t *red,
-                                             uint64_t &computed, bool keep_pred, float *sums = nullptr) {
+                                             uint64_t &computed, bool keep_pred, float *sums = nullptr,
+                                             const LateDt *late = nullptr) {
     const uint32_t tid = threadIdx.x;
     const uint32_t b = it.tile >> 2;
-    if (STAGE == 0 && (it.tile & 3u) == 0u && tid == 0) s.blk[kBlkWords * b + kBlkWet] = 0u;
+    uint32_t late_dt = 0u, late_mark = 0u;
+    if (late && tid == 0) {  // in flight while the fluxes are computed
+        late_dt = *late->dt;
+        late_mark = *late->mark;
+    }
+    if (STAGE == 0 && !late && (it.tile & 3u) == 0u && tid == 0) s.blk[kBlkWords * b + kBlkWet] = 0u;
     const float *C0 = B.c + in_col * kTileCells, *C1 = C0 + kTileCells, *C2 = C0 + 2 * kTileCells;
     const int base = static_cast<int>(it.tile * kTileCells);
     int32_t *live_w = F ? reinterpret_cast<int32_t *>(F) : B.cr;
@@ -314,7 +334,14 @@ __device__ __forceinline__ bool tile_compute(const swe_mesh_t &m, const swe_stat
         W4[j] = w4;
         if (STAGE == 1) W5[j] = __float_as_int(w5);
     }
+    if (late && tid == 0) {
+        const bool active = late->all || late_mark == late->epoch;
+        late->slot[0] = active ? late_dt : 0u;
+        late->slot[1] = late_dt;
+        if (STAGE == 0 && active && late_dt != 0u && (it.tile & 3u) == 0u) s.blk[kBlkWords * b + kBlkWet] = 0u;
+    }
     __syncthreads();
+    if (late) dt = __uint_as_float(late->slot[0]);
 
     bool wet = false;
     uint32_t bound = kNoBound;

@@ -1,4 +1,4 @@
-"""The oracles themselves, pinned to the reference before they judge the CUDA path.
+"""The oracles themselves, pinned to the reference before they check the CUDA path.
 
 * The FP64 oracle (``oracle/fp64_step.py``) must reproduce the reference's
   ``tests/unit/_cpu_step.py`` outputs stored in ``tests/golden/cpu_step.npz``.
