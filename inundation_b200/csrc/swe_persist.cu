@@ -61,7 +61,8 @@ struct SeatShared {
     uint32_t seat_forced;
     uint32_t ring_n;
     uint32_t ring[kRingCache];
-    uint32_t ring_active[kRingCache / 32];  // ring blocks active in this step (seat only)
+    uint32_t ring_active[kRingCache / 32];  // ring blocks active in this step
+    uint32_t ring_ok;         // ring_active holds this step's bits for the seat
     uint32_t qlen;            // tiles queued for this step
     uint32_t take;            // a taken tile (kNoTile: the queue is empty)
     uint4 take_item;
@@ -259,8 +260,12 @@ __device__ bool seat_predictor(const swe_mesh_t &m, const swe_state_t &s, const 
         fence_proxy_async();
         __syncthreads();
     }
-    if (!OPEN && !all_active && ss.seat_active && ss.ring_n <= kRingCache && tid >= 32u && tid < 64u) {
-        // which blocks of the seat's two-ring are active now (read beside the first take)
+    // A seat active from the start of the step keeps its tile all step: which blocks
+    // of its two-ring are active now (read beside the first take). A tile seated
+    // later has no such bits.
+    const bool ring_ok = !OPEN && !all_active && ss.seat_active && ss.ring_n <= kRingCache;
+    if (tid == 0) ss.ring_ok = ring_ok ? 1u : 0u;
+    if (ring_ok && tid >= 32u && tid < 64u) {
         const uint32_t lane = tid & 31u;
         for (uint32_t w = 0; w * 32u < ss.ring_n; ++w) {
             const uint32_t k = w * 32u + lane;
@@ -340,7 +345,7 @@ __device__ bool seat_corrector(const swe_mesh_t &m, const swe_state_t &s, const 
         if (!all_active && tid < 32u && (wet || ss.seat_forced != 0u)) {
             const bool cached = ss.ring_n <= kRingCache;
             mark_ring(m, s, it.tile >> 2, epoch, next, qpar, cached ? ss.ring : nullptr, ss.ring_n,
-                      !OPEN && cached ? ss.ring_active : nullptr);
+                      ss.ring_ok ? ss.ring_active : nullptr);
         }
         fence_proxy_async();
         __syncthreads();

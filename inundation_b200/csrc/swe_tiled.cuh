@@ -241,8 +241,8 @@ struct TiledShared {
 // A predictor started before its dt and the tile's activity are known (the
 // persistent kernel's seat): thread 0 loads both at the start, and after the
 // fluxes, which need neither, publishes in slot[0] the dt the update uses (0
-// when the tile turns out inactive: the update then keeps nothing anyone reads)
-// and in slot[1] the instance's dt.
+// when the tile turns out inactive or its instance does not run: the update is
+// then skipped) and in slot[1] the instance's dt.
 struct LateDt {
     const uint32_t *dt;    // the instance's dt word
     const uint32_t *mark;  // the block's epoch word
@@ -341,7 +341,10 @@ __device__ __forceinline__ bool tile_compute(const swe_mesh_t &m, const swe_stat
         if (STAGE == 0 && active && late_dt != 0u && (it.tile & 3u) == 0u) s.blk[kBlkWords * b + kBlkWet] = 0u;
     }
     __syncthreads();
-    if (late) dt = __uint_as_float(late->slot[0]);
+    if (late) {
+        if (late->slot[0] == 0u) return false;
+        dt = __uint_as_float(late->slot[0]);
+    }
 
     bool wet = false;
     uint32_t bound = kNoBound;
