@@ -124,7 +124,8 @@ typedef struct {
                                       persistent kernel's [10] step epoch, [11] start-list tiles taken and
                                       [12..15] its two tile queues' lengths and taken counts; others zero */
     uint32_t *dt_buf;              /* 4 words per instance: [0] this step's dt (float bits, 0 = no-op),
-                                      [1] the next step's CFL bound */
+                                      [1] the next step's CFL bound, [2..3] the persistent kernel's
+                                      published (dt, step epoch) pair; 16-byte aligned */
     swe_ctrl_t *ctrl;              /* one per instance */
     uint32_t *sync;                /* 64 zeroed words: the grid barrier of the persistent kernel (kernel 2) */
     uint32_t *marks;               /* 2 words per block, zeroed with sched word 10 at the start of a run: word

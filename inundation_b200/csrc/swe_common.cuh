@@ -6,7 +6,8 @@
 // each starting on a block boundary; block_inst names a block's instance,
 // block_cells its real cells. Every instance has its own clock (control
 // block) and its own dt words: dt_buf[4 i] is the dt of its current step
-// (0 = no-op), dt_buf[4 i + 1] the CFL bound reduced for its next step.
+// (0 = no-op), dt_buf[4 i + 1] the CFL bound reduced for its next step,
+// dt_buf[4 i + 2..3] the (dt, step epoch) pair the persistent kernel publishes.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -128,8 +129,17 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
     return true;
 }
 
+__device__ __forceinline__ uint64_t ld_relaxed_u64(const uint64_t *p) {
+    uint64_t v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u64(uint64_t *p, uint64_t v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
 // -- integer-tick step control (resident.py:813-885) ---------------------------------------------
-__device__ __forceinline__ void step_control(swe_ctrl_t *c, uint32_t *dt_buf, int mode) {
+__device__ __forceinline__ uint32_t step_control(swe_ctrl_t *c, uint32_t *dt_buf, int mode) {
     float raw;
     if (mode == 0) {
         raw = __uint_as_float(dt_buf[0]);
@@ -160,8 +170,31 @@ __device__ __forceinline__ void step_control(swe_ctrl_t *c, uint32_t *dt_buf, in
     if (c->dt_max_ticks < ticks) ticks = c->dt_max_ticks;
     if (static_cast<uint64_t>(ticks) > remaining) ticks = static_cast<uint32_t>(remaining);
     c->dt_ticks = ticks;
-    dt_buf[0] = __float_as_uint(static_cast<float>(ticks) / kTicksPerSecond);
+    const uint32_t dt = __float_as_uint(static_cast<float>(ticks) / kTicksPerSecond);
+    dt_buf[0] = dt;
     dt_buf[1] = __float_as_uint(kDtSentinel);
+    return dt;
+}
+
+// The persistent kernel's step control publishes an instance's next dt as the
+// pair (dt, epoch of that step) in dt words 2..3 after it has released the grid.
+// The dt of the step of `epoch` from the pair's value v, read again until the
+// pair carries that epoch (bounded: 0 and error bit 4 when it does not come).
+__device__ __forceinline__ uint32_t published_dt(const swe_state_t &s, const uint64_t *pair, uint32_t epoch,
+                                                 uint64_t v) {
+    if (static_cast<uint32_t>(v >> 32) == epoch) return static_cast<uint32_t>(v);
+    const uint64_t t0 = global_ns();
+    for (;;) {
+        v = ld_relaxed_u64(pair);
+        if (static_cast<uint32_t>(v >> 32) == epoch) return static_cast<uint32_t>(v);
+        if (global_ns() - t0 > kWaitLimitNs) {
+            atomicOr(&s.ctrl->error, 4u);
+            return 0u;
+        }
+    }
+}
+__device__ __forceinline__ const uint64_t *dt_pair(const swe_state_t &s, uint32_t inst) {
+    return reinterpret_cast<const uint64_t *>(s.dt_buf + kDtWords * inst + 2u);
 }
 
 // The state beyond boundary edge cR < 0 from the cell inside it: a wall's

@@ -80,4 +80,41 @@ __device__ __forceinline__ bool grid_sync(GridSync &g, int *flag, F last) {
     return ok;
 }
 
+// grid_sync whose last arriver releases the others first and then runs `after`
+// (all its threads): work that nobody reads before the next barrier, or that the
+// readers wait for by other means.
+template <typename F>
+__device__ __forceinline__ bool grid_sync_then(GridSync &g, int *flag, F after) {
+    fence_proxy_async_global();
+    __syncthreads();
+    uint32_t *const cnt = g.count + 16u * g.parity;
+    if (threadIdx.x == 0) {
+        flag[1] = 1;
+        if (atom_add_acq_rel_gpu(cnt, 1u) == gridDim.x - 1) {
+            flag[0] = 1;
+            *reinterpret_cast<volatile uint32_t *>(cnt) = 0u;
+            red_add_release_gpu(g.gen, 1u);
+        } else {
+            flag[0] = 0;
+            const uint64_t t0 = global_ns();
+            while (ld_acquire_u32(g.gen) == g.epoch) {
+                if (global_ns() - t0 > kWaitLimitNs) {
+                    flag[1] = 0;
+                    break;
+                }
+            }
+        }
+    }
+    g.epoch += 1u;
+    g.parity ^= 1u;
+    __syncthreads();
+    const bool last = flag[0] != 0, ok = flag[1] != 0;
+    if (last) {
+        after();
+        __syncthreads();
+    }
+    fence_proxy_async_global();
+    return ok;
+}
+
 }  // namespace swe

@@ -153,6 +153,15 @@ __device__ __forceinline__ bool seat_wait(const swe_state_t &s, const TileBuf &B
     return false;
 }
 
+// The dt of instance `inst` in step `step` of epoch `epoch`: from the second step
+// of a launch on it is the published pair's (the step control runs after the
+// grid's release).
+__device__ __forceinline__ uint32_t step_dt(const swe_state_t &s, uint32_t inst, uint32_t step, uint32_t epoch) {
+    if (step == 0u) return s.dt_buf[kDtWords * inst];
+    const uint64_t *pair = dt_pair(s, inst);
+    return published_dt(s, pair, epoch, ld_relaxed_u64(pair));
+}
+
 // Take the next tile of this step's queue (thread 0 takes, all threads see it in
 // ss.take / take_item / take_dt): skipped are tiles of instances that do not run
 // this step and, from the second step on, tiles whose block is no longer active
@@ -169,7 +178,7 @@ __device__ __forceinline__ void seat_take(const swe_mesh_t &m, const swe_state_t
             const uint32_t t = step == 0u ? unpack(reinterpret_cast<const uint4 *>(s.items)[idx]).tile
                                           : tile_queue(m, s, step & 1u)[idx];
             const uint32_t b = t >> 2, inst = m.block_inst[b];
-            const uint32_t dt = s.dt_buf[kDtWords * inst];
+            const uint32_t dt = step_dt(s, inst, step, epoch);
             if (dt == 0u) continue;  // a no-op step keeps the block's flags
             const bool active = step == 0u || all_active || s.marks[2u * b] == epoch;
             const uint32_t flag = s.blk[kBlkWords * b + kBlkActive];
@@ -199,7 +208,7 @@ __device__ bool seat_predictor(const swe_mesh_t &m, const swe_state_t &s, const 
     float *F = reinterpret_cast<float *>(smem + L.total);
     const TileBuf B0 = tile_buf(smem, L, 0u), B1 = tile_buf(smem, L, 1u);
     const uint32_t tid = threadIdx.x;
-    if (!OPEN && ss.seat != kNoTile) {
+    if (!OPEN && step > 0u && ss.seat != kNoTile) {
         // The seat's predictor starts before its activity and dt are known: both arrive
         // while its fluxes are computed (the update of an inactive seat keeps nothing
         // anyone reads). An open mesh's tallies need dt in the flux loop: no early start.
@@ -209,7 +218,7 @@ __device__ bool seat_predictor(const swe_mesh_t &m, const swe_state_t &s, const 
             if (tid < 32u) seat_issue<0>(m, s, ss.seat_item, B0, true);
             if (!seat_wait(s, B0, ph, 0u)) return false;
         }
-        const LateDt late{s.dt_buf + kDtWords * it.inst, s.marks + 2u * b, epoch, all_active ? 1u : 0u, sh.late};
+        const LateDt late{dt_pair(s, it.inst), s.marks + 2u * b, epoch, all_active ? 1u : 0u, sh.late};
         tile_compute<0, COMP, CLAMP, kPersistThreads, OPEN>(m, s, p, cfl, B0, it, 0.0f, 0u, 6u, F, L.capE, sh.red,
                                                             computed, true, nullptr, &late);
         fence_proxy_async();
@@ -234,7 +243,7 @@ __device__ bool seat_predictor(const swe_mesh_t &m, const swe_state_t &s, const 
         ss.seat_active = 0u;
         if (ss.seat != kNoTile) {
             const uint32_t b = ss.seat >> 2;
-            const uint32_t dt = s.dt_buf[kDtWords * unpack(ss.seat_item).inst];
+            const uint32_t dt = step_dt(s, unpack(ss.seat_item).inst, step, epoch);
             const bool active = all_active || s.marks[2u * b] == epoch;
             if (dt != 0u && active) {
                 ss.seat_active = 1u;
@@ -438,6 +447,9 @@ __global__ void __launch_bounds__(kPersistThreads, 1024 / kPersistThreads)
             }
         }
     }
+    if (blockIdx.x == 0)  // no published dt pair of an earlier run or launch carries an epoch of this one
+        for (uint32_t i = threadIdx.x; i < m.n_inst; i += blockDim.x)
+            *const_cast<uint64_t *>(dt_pair(s, i)) = 0ull;
     __syncthreads();
     const uint32_t first = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
     const bool all = all_active != 0;
@@ -472,8 +484,8 @@ __global__ void __launch_bounds__(kPersistThreads, 1024 / kPersistThreads)
         const bool last_step = step + 1u == n_steps;
         auto control = [&] {
             for (uint32_t i = threadIdx.x; i < m.n_inst; i += blockDim.x) {
-                s.dt_buf[kDtWords * i + 2u] = s.dt_buf[kDtWords * i];
-                step_control(s.ctrl + i, s.dt_buf + kDtWords * i, 1);
+                const uint32_t dt = step_control(s.ctrl + i, s.dt_buf + kDtWords * i, 1);
+                st_release_u64(const_cast<uint64_t *>(dt_pair(s, i)), (static_cast<uint64_t>(next_epoch) << 32) | dt);
             }
             if (threadIdx.x == blockDim.x - 1u) {  // beside instance 0's control, not after it
                 volatile uint32_t *sched = s.sched;
@@ -491,7 +503,10 @@ __global__ void __launch_bounds__(kPersistThreads, 1024 / kPersistThreads)
                 }
             }
         };
-        if (!(ok = grid_sync(g, flag, control))) break;
+        // The step control runs after the release, the others wait for its dt pairs
+        // only where they need them; the last step's runs before (the hand-over
+        // reads its dt and the lists it zeroes).
+        if (!(ok = last_step ? grid_sync(g, flag, control) : grid_sync_then(g, flag, control))) break;
     }
     if (ok && step > 0u) seat_handover(m, s, epoch0 + step + 1u, all);
     if (threadIdx.x == 0) {
@@ -573,7 +588,7 @@ extern "C" int swe_steps(const swe_mesh_t *mesh, const swe_state_t *state, const
         }
         return SWE_OK;
     }
-    if (!state->sync || !state->marks) return SWE_ERR_ARGUMENT;
+    if (!state->sync || !state->marks || (reinterpret_cast<uintptr_t>(state->dt_buf) & 15u)) return SWE_ERR_ARGUMENT;
     if (mesh->max_sub_edges > 2047u || mesh->max_sub_slots > 2047u || mesh->n_inst > 1023u) return SWE_ERR_TOO_LARGE;
     if (sources->count && (!sources->cells || !sources->rate)) return SWE_ERR_ARGUMENT;
     return mesh->n_open ? dispatch_persistent<true>(mesh, state, params, sources, n_steps, stream)

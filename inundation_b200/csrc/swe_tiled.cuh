@@ -242,11 +242,12 @@ struct TiledShared {
 // persistent kernel's seat): thread 0 loads both at the start, and after the
 // fluxes, which need neither, publishes in slot[0] the dt the update uses (0
 // when the tile turns out inactive or its instance does not run: the update is
-// then skipped) and in slot[1] the instance's dt.
+// then skipped) and in slot[1] the instance's dt. The dt comes from the pair
+// the step control publishes, which may still be on its way.
 struct LateDt {
-    const uint32_t *dt;    // the instance's dt word
+    const uint64_t *dt;    // the instance's published (dt, epoch) pair
     const uint32_t *mark;  // the block's epoch word
-    uint32_t epoch;        // the epoch of an active block
+    uint32_t epoch;        // this step's epoch: of an active block, and of the pair
     uint32_t all;          // every block is active
     uint32_t *slot;        // two shared words
 };
@@ -274,9 +275,10 @@ __device__ __forceinline__ bool tile_compute(const swe_mesh_t &m, const swe_stat
                                              const LateDt *late = nullptr) {
     const uint32_t tid = threadIdx.x;
     const uint32_t b = it.tile >> 2;
-    uint32_t late_dt = 0u, late_mark = 0u;
+    uint64_t late_pair = 0u;
+    uint32_t late_mark = 0u;
     if (late && tid == 0) {  // in flight while the fluxes are computed
-        late_dt = *late->dt;
+        late_pair = ld_relaxed_u64(late->dt);
         late_mark = *late->mark;
     }
     if (STAGE == 0 && !late && (it.tile & 3u) == 0u && tid == 0) s.blk[kBlkWords * b + kBlkWet] = 0u;
@@ -335,6 +337,7 @@ __device__ __forceinline__ bool tile_compute(const swe_mesh_t &m, const swe_stat
         if (STAGE == 1) W5[j] = __float_as_int(w5);
     }
     if (late && tid == 0) {
+        const uint32_t late_dt = published_dt(s, late->dt, late->epoch, late_pair);
         const bool active = late->all || late_mark == late->epoch;
         late->slot[0] = active ? late_dt : 0u;
         late->slot[1] = late_dt;

@@ -414,7 +414,8 @@ class ResidentEngine:
         self._active_blocks = int(self._sched_pinned.numpy().view(np.uint32)[0])
         err = int(self._ctrl["error"].max())
         if err:
-            what = {1: "for staged data", 2: "at a grid barrier"}.get(err & 3, "")
+            what = " and ".join(w for bit, w in ((1, "for staged data"), (2, "at a grid barrier"),
+                                                   (4, "for a step's dt")) if err & bit)
             raise RuntimeError(f"{B200_BACKEND}: a bounded device wait {what} timed out (error {err})")
 
     def _enqueue_prologue(self) -> None:
