@@ -66,6 +66,30 @@ def test_status_strings_and_argument_checks(lib: ctypes.CDLL) -> None:
     assert lib.swe_configure(None, 0, None) == 1
 
 
+def test_whole_steps_refuse_a_misaligned_dt_buffer(lib: ctypes.CDLL) -> None:
+    """Kernel 2 publishes each dt as a 64-bit pair in dt words 2..3: dt_buf must be 16-byte aligned.
+
+    The structs carry placeholder addresses that nothing dereferences: the argument
+    checks run on the host before any device call.
+    """
+    mesh = native.SweMesh(n_cells=256, n_blocks=1, max_tile_edges=64, n_inst=1, max_sub_edges=64, max_sub_slots=64)
+    for name, kind in native.SweMesh._fields_:
+        if kind is native._P and name != "open_cond":
+            setattr(mesh, name, 0x10000)
+    state = native.SweState(**{name: 0x20000 for name, _ in native.SweState._fields_})
+    params = native.SweParams(g=9.81, dry_tol=1e-4, cfl=0.8, compensated=1, active_set=1, kernel=2)
+    sources = native.SweSources()
+    state.dt_buf = 0x20008
+    assert lib.swe_steps(ctypes.byref(mesh), ctypes.byref(state), ctypes.byref(params), ctypes.byref(sources), 1,
+                         None) == 1
+    import torch
+
+    if not torch.cuda.is_available():  # with a device, an aligned buffer would launch on the placeholders
+        state.dt_buf = 0x20010
+        assert lib.swe_steps(ctypes.byref(mesh), ctypes.byref(state), ctypes.byref(params), ctypes.byref(sources),
+                             1, None) == 2  # past the argument checks: the CUDA runtime finds no device
+
+
 def test_ctypes_structs_match_the_header_layout() -> None:
     assert ctypes.sizeof(native.SweMesh) == 16 + 17 * 8 + 8 + 11 * 8 + 8 + 8  # n_open (padded), open_cond
     assert native.SweMesh.n_open.offset == 248 and native.SweMesh.open_cond.offset == 256
