@@ -59,8 +59,31 @@ __device__ __forceinline__ void source_apply(const swe_mesh_t &m, const swe_stat
     }
 }
 
+// One instance's CFL bound from a warp: every lane's (inst, bound), kNoBound for
+// none. A warp whose bounds all belong to one instance sends one atomic minimum;
+// otherwise every lane sends its own. Called by all 32 lanes.
+__device__ __forceinline__ void bound_flush_warp(const swe_state_t &s, uint32_t inst, uint32_t bound) {
+    constexpr unsigned kFull = 0xFFFFFFFFu;
+    const bool has = bound != kNoBound;
+    const unsigned with = __ballot_sync(kFull, has);
+    if (!with) return;
+    const int leader = __ffs(with) - 1;
+    const uint32_t ref = __shfl_sync(kFull, inst, leader);
+    if (__all_sync(kFull, !has || inst == ref)) {
+        const uint32_t low = __reduce_min_sync(kFull, bound);
+        if (static_cast<int>(threadIdx.x & 31u) == leader) atomicMin(&s.dt_buf[kDtWords * ref + 1], low);
+    } else if (has) {
+        atomicMin(&s.dt_buf[kDtWords * inst + 1], bound);
+    }
+}
+
+// The post-source CFL bounds: each thread keeps the minimum of its sources'
+// bounds while they belong to one instance, and the warp combines them at the
+// end, so the dt word sees few atomics however many sources there are (a
+// minimum is the same in any order). Called by every thread of whole warps.
 __device__ __forceinline__ void source_bound(const swe_mesh_t &m, const swe_state_t &s, const swe_sources_t &src,
                                              const Phys &p, float cfl, uint32_t first, uint32_t stride) {
+    uint32_t acc_inst = 0u, acc = kNoBound;
     for (uint32_t k = first; k < src.count; k += stride) {
         const uint32_t i = src.cells[k];
         const uint32_t inst = m.block_inst[i >> 8];
@@ -79,8 +102,16 @@ __device__ __forceinline__ void source_bound(const swe_mesh_t &m, const swe_stat
             lam += (u + (dry_side ? 2.0f : 1.0f) * c) * m.tile_len[e];
         }
         const float A = m.area[i];
-        if (lam > 1e-30f && A > 1e-10f) atomicMin(&s.dt_buf[kDtWords * inst + 1], __float_as_uint(cfl * A / lam));
+        if (!(lam > 1e-30f && A > 1e-10f)) continue;
+        const uint32_t b = __float_as_uint(cfl * A / lam);
+        if (inst != acc_inst && acc != kNoBound) {
+            atomicMin(&s.dt_buf[kDtWords * acc_inst + 1], acc);
+            acc = kNoBound;
+        }
+        acc_inst = inst;
+        acc = min(acc, b);
     }
+    bound_flush_warp(s, acc_inst, acc);
 }
 
 }  // namespace swe
