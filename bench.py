@@ -19,6 +19,13 @@ wet blocks are skipped, as in the reference's resident backend).
 * ``cpu_baseline``: the float64 oracle step timed on one host core on the
   same mesh; its result also gives the stated float64 error of the CUDA step.
 
+Other workloads (``--workload``): ``full_wet`` and ``one_cell`` on the same
+mesh (every block active; a single wet cell), ``lake_at_rest`` (8k cells over
+1 km, six Gaussian bumps under a 1 m surface, CFL 0.9) and ``rain_inflow``
+(4M cells over 20 km, 40 m relief, n log-uniform in [0.02, 0.08], 50 mm/h
+rain on every cell plus a triangular inflow of 200 m^3/s peak; timed after a
+spin-up in which the rain wets the mesh).
+
 ``--impl reference`` times the reference's CPU step (its float64 NumPy
 restatement) on all host cores instead; under torchrun only rank 0 works.
 With N GPUs every rank runs an independent replica (the single-mesh path
@@ -46,6 +53,14 @@ METRIC = "cell-steps/s fwd and fwd+adjoint, plain vs batched, at stated FP64-ora
 UNIT = "cell-steps/s"
 L2_BYTES = 126 * 2**20
 SENTINEL_STOP = 1 << 62
+# workload: default cells and seed
+WORKLOADS = {
+    "dam_break": (1_000_000, 2),
+    "full_wet": (1_000_000, 2),
+    "one_cell": (1_000_000, 2),
+    "lake_at_rest": (8_000, 1),
+    "rain_inflow": (4_000_000, 3),
+}
 
 
 def parse_args() -> argparse.Namespace:
@@ -54,9 +69,9 @@ def parse_args() -> argparse.Namespace:
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=["dam_break", "full_wet", "one_cell"], default="dam_break")
-    ap.add_argument("--cells", type=int, default=1_000_000)
-    ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="dam_break")
+    ap.add_argument("--cells", type=int, default=None, help="mesh cells (default: the workload's)")
+    ap.add_argument("--seed", type=int, default=None, help="mesh and terrain seed (default: the workload's)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--chunk", type=int, default=500, help="steps per captured graph in the timed region")
@@ -69,13 +84,23 @@ def parse_args() -> argparse.Namespace:
     ap.add_argument("--no-adjoint", action="store_true", help="skip the forward+adjoint measurement")
     ap.add_argument("--adjoint-cells", type=int, default=250_000)
     ap.add_argument("--adjoint-steps", type=int, default=2000)
-    return ap.parse_args()
+    ap.add_argument("--spin-up", type=float, default=60.0,
+                    help="rain_inflow: simulated seconds run before the timed steps")
+    args = ap.parse_args()
+    cells, seed = WORKLOADS[args.workload]
+    args.cells = cells if args.cells is None else args.cells
+    args.seed = seed if args.seed is None else args.seed
+    return args
 
 
 # -- workload ----------------------------------------------------------------------------------
 def build_scenario(name: str, cells: int, seed: int):
     from inundation_b200 import scenarios
 
+    if name == "lake_at_rest":
+        return scenarios.lake_at_rest(cells, seed=seed, side=1000.0 * np.sqrt(cells / 8000))
+    if name == "rain_inflow":
+        return scenarios.rain_inflow(cells, seed=seed, side=20_000.0 * np.sqrt(cells / 4_000_000))
     side = 10_000.0 * np.sqrt(cells / 1_000_000)
     sc = scenarios.dam_break(cells, seed=seed, side=side)
     if name == "full_wet":
@@ -95,26 +120,42 @@ def build_scenario(name: str, cells: int, seed: int):
     return sc
 
 
-def workload_config(sc, args) -> dict:
+WORKLOAD_TEXT = {
+    "dam_break": {"terrain": "fractal beta 2, 20 m relief, 3 m channel",
+                  "water": "4 m depth within 500 m of the centre, dry outside", "manning_n": 0.035},
+    "full_wet": {"terrain": "fractal beta 2, 20 m relief, 3 m channel", "water": "still water + current, all wet",
+                 "manning_n": 0.035},
+    "one_cell": {"terrain": "fractal beta 2, 20 m relief, 3 m channel", "water": "one wet cell (1 m), dry elsewhere",
+                 "manning_n": 0.035},
+    "lake_at_rest": {"terrain": "six Gaussian bumps (0.2-0.8 m, sigma 50-150 m) on a flat bed",
+                     "water": "still surface at 1 m, zero momentum", "manning_n": 0.03},
+    "rain_inflow": {"terrain": "fractal beta 2, 40 m relief, 3 m channel",
+                    "water": "initially dry; 50 mm/h rain on every cell, triangular inflow (200 m^3/s at 20 min) "
+                             "at the highest cell", "manning_n": "log-uniform in [0.02, 0.08]"},
+}
+
+
+def workload_config(sc, args, cfl: float = 0.8) -> dict:
     g = sc.geom
     from inundation_b200.layout import algorithmic_bytes_per_cell_step
 
     per_step = algorithmic_bytes_per_cell_step(g) * g.N
+    l2 = (f"inputs larger than L2: {per_step / 2**20:.0f} MiB algorithmic traffic per full step, "
+          f"{L2_BYTES // 2**20} MiB L2; no flush") if per_step > L2_BYTES else (
+          f"inputs fit in L2 ({per_step / 2**20:.1f} MiB algorithmic traffic per full step, "
+          f"{L2_BYTES // 2**20} MiB L2): latency-bound steps, no flush")
     return {
         "workload": f"{sc.name}_{g.N // 1000}k_voronoi",
         "cells": int(g.N),
         "edges": int(g.E),
         "csr_slots": int(g.cell_edge_ptr[-1]),
         "max_degree": int(g.max_degree),
-        "terrain": "fractal beta 2, 20 m relief, 3 m channel",
-        "dam": "4 m depth within 500 m of the centre" if sc.name == "dam_break" else "still water + current, all wet",
-        "manning_n": 0.035,
-        "cfl": 0.8,
+        **WORKLOAD_TEXT.get(sc.name, {}),
+        "cfl": cfl,
         "active_set": True,
         "compensated": True,
         "seed": args.seed,
-        "l2": f"inputs larger than L2: {per_step / 2**20:.0f} MiB algorithmic traffic per full step, "
-        f"{L2_BYTES // 2**20} MiB L2; no flush",
+        "l2": l2,
         "parallelism": f"replicas{args.gpus}" if args.gpus > 1 else "single",
     }
 
@@ -318,11 +359,17 @@ def run_b200(args, world: int, rank: int, local: int) -> None:
 
     device = f"cuda:{local}"
     torch.cuda.set_device(local)
+    if args.workload == "rain_inflow":
+        run_sources_workload(args, world, rank, local)
+        return
     sc = build_scenario(args.workload, args.cells, args.seed)
     g = sc.geom
-    solver = SWESolverB200Resident(g, None, sc.h0, sc.hu0, sc.hv0, sc.manning, dry_tol=sc.dry_tol, device=device)
+    cfl = float(sc.meta.get("cfl", 0.8))
+    solver = SWESolverB200Resident(g, None, sc.h0, sc.hu0, sc.hv0, sc.manning, dry_tol=sc.dry_tol, cfl=cfl,
+                                   device=device)
     solver.stage_kernel = args.kernel
     solver.ctas_per_sm = args.ctas_per_sm
+    v0 = solver.volume_fp64() if args.workload == "lake_at_rest" else None
     plan(solver, sc)
     if args.kernel == "auto":  # the choice "auto" makes for this state, fixed for the timed region
         from inundation_b200.engine import KERNELS
@@ -395,7 +442,7 @@ def run_b200(args, world: int, rank: int, local: int) -> None:
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic: seeded Voronoi mesh, fractal DEM (no real DEM or mesh files)",
-        "config": workload_config(sc, args),
+        "config": workload_config(sc, args, cfl),
         "mode": "forward, plain (one mesh per GPU)",
         "computed_cell_steps_per_s": world * computed / (ms_max * 1e-3),
         "active_fraction": computed / (g.N * args.steps),
@@ -418,6 +465,14 @@ def run_b200(args, world: int, rank: int, local: int) -> None:
         },
         "clocks": clock,
     }
+    if v0 is not None:  # the reference's gate: |u| over cells deeper than 10 dry_tol, float64 volume drift
+        h, hu, hv = solver.download_h(), solver.download_hu(), solver.download_hv()
+        wet = h > 10 * sc.dry_tol
+        line["lake_at_rest_check"] = {
+            "steps_before_check": args.warmup + args.steps,
+            "max_abs_u_mps": float(max((np.abs(hu[wet]) / h[wet]).max(), (np.abs(hv[wet]) / h[wet]).max())),
+            "volume_drift_rel": abs(solver.volume_fp64() - v0) / v0,
+        }
     if rank == 0 and not args.no_e2e:
         line["e2e"] = e2e_run(solver, sc, t_sim, args)
     if rank == 0 and not args.no_cpu_baseline and world == 1:
@@ -463,6 +518,137 @@ def e2e_run(solver, sc, t_sim: float, args) -> dict:
         "d2h_bytes_per_step": (24 * n + 48 * (submits + 1)) / steps,
         "path": "SWESolverB200Resident.reset(host h, hu, hv) + run(t_end) + download_h/hu/hv",
     }
+
+
+def run_sources_workload(args, world: int, rank: int, local: int) -> None:
+    """Rain on every cell plus an inflow hydrograph: the sparse-sources path, timed after a spin-up.
+
+    One ``BatchedSolver`` instance (the solver that takes hydrographs). The mesh
+    starts dry; the timed steps begin once ``--spin-up`` simulated seconds have
+    run, by when the rain has wetted it. The end-to-end run uploads that state
+    from host arrays, restarts the clock and runs the same number of steps.
+    """
+    import torch
+
+    from inundation_b200.batch import BatchedSolver, BatchMember
+    from inundation_b200.engine import KERNELS
+    from inundation_b200.layout import algorithmic_bytes_per_cell_step
+
+    device = f"cuda:{local}"
+    t_build = time.perf_counter()
+    sc = build_scenario(args.workload, args.cells, args.seed)
+    t_build = time.perf_counter() - t_build
+    g = sc.geom
+    member = BatchMember(g, sc.h0, sc.hu0, sc.hv0, sc.manning, source_rate=sc.source_rate,
+                         hydrographs=sc.hydrographs)
+    solver = BatchedSolver([member], dry_tol=sc.dry_tol, device=device)
+    solver.stage_kernel = args.kernel
+    solver.ctas_per_sm = args.ctas_per_sm
+    solver.start(sc.dt_max, sc.dt_init)
+    spin_steps = 0
+    while float(solver.sim_time[0]) < args.spin_up:
+        solver.run_steps(solver.steps_per_graph)
+        spin_steps += solver.steps_per_graph
+        if spin_steps > 200_000:
+            raise RuntimeError("the spin-up did not reach its simulated time")
+    t_spun = float(solver.sim_time[0])
+    spun = {name: solver.download_state(name) for name in ("h", "hu", "hv")}
+    if args.kernel == "auto":  # the choice "auto" makes for this state, fixed for the timed region
+        solver.stage_kernel = {v: k for k, v in KERNELS.items()}[solver._kernel]
+    kernel = solver.stage_kernel
+    _timed_steps(solver, args.warmup, max(1, args.warmup))
+    computed0 = solver.computed_cells
+    steps0 = solver.steps.copy()
+    t0_sim = float(solver.sim_time[0])
+    clocks = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    ms = _timed_steps(solver, args.steps, args.chunk)
+    clock = clocks.stop()
+    barrier(world)
+    ms_max = reduce_max(ms, world)
+    done = solver.steps - steps0
+    if int(done[0]) != args.steps:
+        raise RuntimeError(f"timed region ran {int(done[0])} real steps, expected {args.steps}")
+    computed = solver.computed_cells - computed0
+    t_sim = float(solver.sim_time[0]) - t0_sim
+    bpc = algorithmic_bytes_per_cell_step(g)
+    peak, peak_kind = peaks()
+    achieved = computed * bpc / (ms * 1e-3) / 1e9
+    stage_launches = 2 * args.steps if kernel != "persistent" else -(-args.steps // args.chunk)
+    traffic = None
+    tfile = ROOT / "profiles" / "stage_kernel_traffic.json"
+    if tfile.exists():
+        per_cell = json.loads(tfile.read_text()).get(kernel, {}).get("dram_bytes_per_computed_cell_step")
+        if per_cell:
+            traffic = per_cell * computed / stage_launches
+    per_step_launches = {"persistent": 0, "plain": 5, "tiled": 5}[kernel]  # stages, sources (2), dilation
+
+    # End to end through the public calls: the spun-up state from host arrays, a clock restart, the
+    # same number of steps (the timed region's graphs, already captured), the final depth back.
+    zeros = np.zeros(g.N, np.float32)
+    solver._stream.synchronize()
+    t0 = time.perf_counter()
+    for name in ("h", "hu", "hv"):
+        solver.upload_state(name, spun[name])
+    solver.upload_state("h_lo", zeros)
+    solver.start(sc.dt_max, sc.dt_init)
+    e2e_steps0 = solver.steps.copy()
+    solver.run_steps(args.steps)
+    final_h = solver.download_h(0)
+    e2e_done = int((solver.steps - e2e_steps0)[0])
+    e2e_wall = time.perf_counter() - t0
+    del final_h
+    line = {
+        "metric": METRIC,
+        "value": world * g.N * args.steps / (ms_max * 1e-3),
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic: seeded Voronoi mesh, fractal DEM, seeded roughness (no real DEM or mesh files)",
+        "config": {**workload_config(sc, args), "spin_up_s": t_spun, "spin_up_steps": spin_steps,
+                   "sources": int(np.count_nonzero(sc.source_rate)), "hydrographs": len(sc.hydrographs)},
+        "mode": "forward with sources, plain (one mesh per GPU)",
+        "computed_cell_steps_per_s": world * computed / (ms_max * 1e-3),
+        "active_fraction": computed / (g.N * args.steps),
+        "simulated_s": t_sim,
+        "gpu_launches": per_step_launches * args.steps if kernel != "persistent" else stage_launches,
+        "roofline": {
+            "bound": "hbm",
+            "achieved": achieved,
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": achieved / peak,
+            "traffic": traffic,
+            "kernel": f"whole step ({kernel} stage kernel, sources, dilation): algorithmic bytes of the stages "
+                      "over the step time",
+            "algorithmic_bytes_per_cell_step": bpc,
+            "launches": stage_launches,
+            "peak_kind": f"{peak_kind} HBM copy bandwidth",
+        },
+        "clocks": clock,
+        "e2e": {
+            "value": g.N * e2e_done / e2e_wall,
+            "unit": UNIT,
+            "steps": e2e_done,
+            "wall_s": e2e_wall,
+            "h2d_bytes_per_step": (16 * g.N + 48) / max(e2e_done, 1),
+            "d2h_bytes_per_step": (4 * g.N + 3 * (48 + 64)) / max(e2e_done, 1),
+            "path": "BatchedSolver.upload_state(host h, hu, hv, h_lo) + start + run_steps + download_h",
+        },
+        "build_s": t_build,
+    }
+    del solver
+    torch.cuda.empty_cache()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 # -- batched scenarios -------------------------------------------------------------------------------
