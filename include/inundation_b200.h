@@ -127,7 +127,8 @@ typedef struct {
                                       [1] the next step's CFL bound, [2..3] the persistent kernel's
                                       published (dt, step epoch) pair; 16-byte aligned */
     swe_ctrl_t *ctrl;              /* one per instance */
-    uint32_t *sync;                /* 64 zeroed words: the grid barrier of the persistent kernel (kernel 2) */
+    uint32_t *sync;                /* 64 zeroed words: the grid barrier of the persistent kernel (kernel 2;
+                                      each launch zeroes word 0, its arrival counter, before it starts) */
     uint32_t *marks;               /* 2 words per block, zeroed with sched word 10 at the start of a run: word
                                       0 the epoch of the latest step the block is active in (kernel 2), word
                                       1 unused */
@@ -172,7 +173,8 @@ typedef struct {
 } swe_sources_t;
 
 /* n_steps whole steps: swe_step n_steps times (kernel 0 or 1), or one persistent cooperative launch
-   running them all (kernel 2; params->grid caps its CTAs, 0 = as many as fit). A wait of the
+   running them all (kernel 2; params->grid caps its CTAs, 0 = as many as fit; status 3 when
+   (4 n_steps + 1) x CTAs reaches 2^32, the range of its barrier counter). A wait of the
    persistent kernel that times out records error 2 in the control block. */
 int swe_steps(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params_t *params,
               const swe_sources_t *sources, uint32_t n_steps, swe_stream_t stream);

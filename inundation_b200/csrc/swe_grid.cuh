@@ -80,24 +80,31 @@ __device__ __forceinline__ bool grid_sync(GridSync &g, int *flag, F last) {
     return ok;
 }
 
-// grid_sync whose last arriver releases the others first and then runs `after`
-// (all its threads): work that nobody reads before the next barrier, or that the
-// readers wait for by other means.
+// Grid-wide barrier on one arrival counter, zeroed before the launch: barrier k
+// of the launch completes when the counter reaches (k + 1) x CTAs, and every
+// CTA waits on the counter itself, so the others go on as soon as the last
+// arrival lands (no separate release word to write and see). The last arriver,
+// which learns it from its add, then runs `after` (all its threads): work that
+// nobody reads before the next barrier, or that the readers wait for by other
+// means. Acquire-release adds on one location form one release sequence, so a
+// CTA that reads the full count has acquired every arrival's writes.
+struct CountSync {
+    uint32_t *count;  // arrivals in this launch
+    uint32_t target;  // arrivals that complete the next barrier
+};
+
 template <typename F>
-__device__ __forceinline__ bool grid_sync_then(GridSync &g, int *flag, F after) {
+__device__ __forceinline__ bool count_sync(CountSync &g, int *flag, F after) {
     fence_proxy_async_global();
     __syncthreads();
-    uint32_t *const cnt = g.count + 16u * g.parity;
+    g.target += gridDim.x;
     if (threadIdx.x == 0) {
         flag[1] = 1;
-        if (atom_add_acq_rel_gpu(cnt, 1u) == gridDim.x - 1) {
-            flag[0] = 1;
-            *reinterpret_cast<volatile uint32_t *>(cnt) = 0u;
-            red_add_release_gpu(g.gen, 1u);
-        } else {
-            flag[0] = 0;
+        const uint32_t old = atom_add_acq_rel_gpu(g.count, 1u);
+        flag[0] = old + 1u == g.target ? 1 : 0;
+        if (old + 1u != g.target) {
             const uint64_t t0 = global_ns();
-            while (ld_acquire_u32(g.gen) == g.epoch) {
+            while (ld_acquire_u32(g.count) < g.target) {
                 if (global_ns() - t0 > kWaitLimitNs) {
                     flag[1] = 0;
                     break;
@@ -105,8 +112,6 @@ __device__ __forceinline__ bool grid_sync_then(GridSync &g, int *flag, F after) 
             }
         }
     }
-    g.epoch += 1u;
-    g.parity ^= 1u;
     __syncthreads();
     const bool last = flag[0] != 0, ok = flag[1] != 0;
     if (last) {

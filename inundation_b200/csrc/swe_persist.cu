@@ -431,12 +431,11 @@ __global__ void __launch_bounds__(kPersistThreads, 1024 / kPersistThreads)
     __shared__ SeatShared ss;
     __shared__ int flag[2];
     __shared__ uint32_t epoch0;
-    GridSync g{s.sync, s.sync + 32, 0u, 0u};
+    CountSync g{s.sync, 0u};  // the launch zeroes the counter before the kernel starts
     if (threadIdx.x == 0) {
         mbar_init(reinterpret_cast<uint64_t *>(smem), 1u);
         mbar_init(reinterpret_cast<uint64_t *>(smem) + 1, 1u);
         fence_barrier_init();
-        g.epoch = ld_acquire_u32(g.gen);
         epoch0 = *reinterpret_cast<volatile uint32_t *>(s.sched + kSchedEpoch);  // before any CTA's first barrier
         ss.seat = ss.staged = kNoTile;
         ss.state_ok = 0u;
@@ -465,13 +464,13 @@ __global__ void __launch_bounds__(kPersistThreads, 1024 / kPersistThreads)
         if (!(ok = seat_predictor<COMP, CLAMP, OPEN>(m, s, p, cfl, smem, sh, ss, ph, computed, step, epoch, all,
                                                       src.count != 0u)))
             break;
-        if (!(ok = grid_sync(g, flag, nothing))) break;
+        if (!(ok = count_sync(g, flag, nothing))) break;
         if (!(ok = seat_corrector<COMP, CLAMP, OPEN>(m, s, p, cfl, smem, sh, ss, ph, computed, step, epoch, all)))
             break;
         if (src.count) {
-            if (!(ok = grid_sync(g, flag, nothing))) break;
+            if (!(ok = count_sync(g, flag, nothing))) break;
             source_apply(m, s, src, p.dry_tol, COMP ? 1 : 0, first, stride);
-            if (!(ok = grid_sync(g, flag, nothing))) break;
+            if (!(ok = count_sync(g, flag, nothing))) break;
             source_bound(m, s, src, p, cfl, first, stride);
             if (!all) {  // a source that wets its block marks the block's two-ring
                 for (uint32_t q = first; q < src.count; q += stride) {
@@ -504,9 +503,10 @@ __global__ void __launch_bounds__(kPersistThreads, 1024 / kPersistThreads)
             }
         };
         // The step control runs after the release, the others wait for its dt pairs
-        // only where they need them; the last step's runs before (the hand-over
-        // reads its dt and the lists it zeroes).
-        if (!(ok = last_step ? grid_sync(g, flag, control) : grid_sync_then(g, flag, control))) break;
+        // only where they need them.
+        if (!(ok = count_sync(g, flag, control))) break;
+        // the hand-over reads the last step's dt and the lists its control zeroes
+        if (last_step && !(ok = count_sync(g, flag, nothing))) break;
     }
     if (ok && step > 0u) seat_handover(m, s, epoch0 + step + 1u, all);
     if (threadIdx.x == 0) {
@@ -532,6 +532,8 @@ int launch_persistent(const swe_mesh_t *m, const swe_state_t *s, const swe_param
     const uint32_t grid = (p->grid == 0u || p->grid > fit) ? fit : p->grid;
     // every tile of a step must find a CTA: one seat and kExtraCap others each
     if (4ull * m->n_blocks > static_cast<uint64_t>(grid) * (1u + kExtraCap)) return SWE_ERR_TOO_LARGE;
+    // the barrier's arrival counter (at most four barriers a step, one more at the end) stays below 2^32
+    if ((4ull * n_steps + 1ull) * grid >= (1ull << 32)) return SWE_ERR_TOO_LARGE;
     Phys ph{p->g, p->dry_tol};
     float cfl = p->cfl;
     int all_active = p->active_set ? 0 : 1;
@@ -539,6 +541,8 @@ int launch_persistent(const swe_mesh_t *m, const swe_state_t *s, const swe_param
     swe_state_t ss = *s;
     swe_sources_t sc = *src;
     void *args[] = {&mm, &ss, &sc, &ph, &cfl, &all_active, &n_steps};
+    // the grid barrier's arrival counter starts from zero in every launch
+    if (cudaMemsetAsync(s->sync, 0, sizeof(uint32_t), st) != cudaSuccess) return SWE_ERR_CUDA;
     if (cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(kern), dim3(grid), dim3(kPersistThreads), args, bytes,
                                     st) != cudaSuccess)
         return SWE_ERR_CUDA;
