@@ -925,16 +925,19 @@ def run_adjoint(args, world: int, local: int) -> dict:
 _WORKER: dict = {}
 
 
-def _ref_worker_init(cells: int, seed: int) -> None:
+def _ref_worker_init(workload: str, cells: int, seed: int, spin_up: float) -> None:
     os.environ["OMP_NUM_THREADS"] = "1"
     sys.path.insert(0, str(ROOT))
-    from inundation_b200 import scenarios
     from oracle import fp64_step
 
-    side = 10_000.0 * np.sqrt(cells / 1_000_000)
-    sc = scenarios.dam_break(cells, seed=seed, side=side)
+    sc = build_scenario(workload, cells, seed)  # the workload at the sample's size, same cell size
+    if workload == "rain_inflow":
+        # the timed CUDA steps start from a mesh the rain has wetted: a film of the rain's depth by then
+        # (the float64 step has no source term)
+        sc.h0 = np.full(sc.geom.N, sc.meta["rain_m_per_s"] * spin_up, np.float32)
     s = fp64_step.State(*(a.astype(np.float64) for a in (sc.h0, sc.hu0, sc.hv0)))
-    dt = min(fp64_step.cfl_dt(sc.geom, s, g=9.81, dry_tol=sc.dry_tol, cfl=0.8), 1.0)
+    cfl = float(sc.meta.get("cfl", 0.8))
+    dt = min(fp64_step.cfl_dt(sc.geom, s, g=9.81, dry_tol=sc.dry_tol, cfl=cfl), sc.dt_max)
     _WORKER.update(geom=sc.geom, state=s, n=sc.manning.astype(np.float64), dt=dt, dry=sc.dry_tol)
 
 
@@ -956,7 +959,8 @@ def run_reference(args, world: int, rank: int) -> None:
     per_core_rate = 3.0e5
     cells = int(np.clip(budget_s * per_core_rate / (args.steps + args.warmup), 2000, args.cells))
     ctx = mp.get_context("spawn")
-    with ctx.Pool(procs, initializer=_ref_worker_init, initargs=(cells, args.seed)) as pool:
+    with ctx.Pool(procs, initializer=_ref_worker_init,
+                  initargs=(args.workload, cells, args.seed, args.spin_up)) as pool:
         for _ in range(args.warmup):
             pool.map(_ref_worker_step, range(procs), chunksize=1)
         t0 = time.perf_counter()
@@ -966,7 +970,7 @@ def run_reference(args, world: int, rank: int) -> None:
         wall = time.perf_counter() - t0
     value = total / wall
     sc_cfg = {
-        "workload": f"dam_break_{args.cells // 1000}k_voronoi",
+        "workload": f"{args.workload}_{args.cells // 1000}k_voronoi",
         "cells": args.cells,
         "sample_cells_per_process": cells,
         "parallelism": f"{procs} processes",
@@ -993,7 +997,10 @@ def run_reference(args, world: int, rank: int) -> None:
             "cores": procs,
             "kind": "port",
             "sample": f"each step: one float64 Heun step of a {cells}-cell sample of the workload (same cell "
-            f"size, terrain and dam) in each of {procs} processes",
+            f"size, terrain and water) in each of {procs} processes"
+            + (f"; rain_inflow: a {1000 * 0.05 / 3600 * args.spin_up:.2f} mm film for the state the rain leaves "
+               f"after {args.spin_up:g} s (the float64 step has no source term)" if args.workload == "rain_inflow"
+               else ""),
         },
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
