@@ -1,0 +1,64 @@
+"""The ``stage_kernel = "auto"`` rule and the persistent kernel's capacity, on a stub engine (no device).
+
+The rule: the persistent whole-step kernel while at most a quarter of the blocks
+are active, or while every active 64-cell tile has a CTA of its grid to itself
+(a small mesh); the 256-cell block kernel otherwise, and always when the
+persistent grid cannot hold a step (one seat and 512 other tiles per CTA).
+"""
+
+from __future__ import annotations
+
+import pytest
+
+from inundation_b200.engine import KERNELS, PERSISTENT_EXTRA_TILES, ResidentEngine
+
+PERSISTENT, PLAIN = KERNELS["persistent"], KERNELS["plain"]
+
+
+def engine(n_blocks: int, active: int, sms: int = 148, per_sm: int = 4, max_grid: int | None = None):
+    e = ResidentEngine.__new__(ResidentEngine)  # the rule reads only these fields
+    e.stage_kernel = "auto"
+    e.n_blocks = n_blocks
+    e._active_blocks = active
+    e._sms = sms
+    e._per_sm = {k: per_sm for k in KERNELS.values()}
+    e.ctas_per_sm = None
+    e.max_grid = max_grid
+    return e
+
+
+@pytest.mark.parametrize(
+    ("n_blocks", "active", "want"),
+    [
+        (3907, 140, PERSISTENT),  # 1M-cell dam break: 3.6 % of the blocks
+        (3907, 976, PERSISTENT),  # a quarter active (976.75), no more
+        (3907, 977, PLAIN),  # past a quarter: issue-bound work for the block kernel
+        (3907, 3907, PLAIN),  # all wet
+        (32, 32, PERSISTENT),  # 8k-cell lake at rest: 128 tiles, one CTA each
+        (148, 148, PERSISTENT),  # 592 tiles on 592 CTAs
+        (149, 149, PLAIN),  # one tile more than CTAs, all active
+    ],
+)
+def test_auto_rule(n_blocks: int, active: int, want: int) -> None:
+    assert engine(n_blocks, active)._kernel == want
+
+
+def test_persistent_needs_room_for_every_tile() -> None:
+    grid = 148 * 4
+    fits = grid * (1 + PERSISTENT_EXTRA_TILES) // 4
+    assert engine(fits, 1)._persistent_fits
+    assert engine(fits, 1)._kernel == PERSISTENT
+    too_many = fits + 1
+    assert not engine(too_many, 1)._persistent_fits
+    assert engine(too_many, 1)._kernel == PLAIN  # sparse, but a step could not find every tile a CTA
+    # a capped grid shrinks both the capacity and the "one CTA per tile" case
+    assert engine(32, 32, max_grid=64)._kernel == PLAIN
+
+
+def test_explicit_choice_and_unknown_names() -> None:
+    e = engine(3907, 3907)
+    e.stage_kernel = "persistent"
+    assert e._kernel == PERSISTENT
+    e.stage_kernel = "fastest"
+    with pytest.raises(ValueError, match="stage_kernel"):
+        _ = e._kernel
