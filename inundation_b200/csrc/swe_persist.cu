@@ -32,8 +32,14 @@ namespace swe {
 // take queued tiles first and seat the first one; a CTA with a seat takes more
 // only after computing its seat, and streams those through its second buffer.
 // A sparse step's critical path is then a few dependent global accesses (the
-// seat's activity mark, the neighbours' states, the two barriers); a dense step
-// spreads the queue over all CTAs.
+// neighbours' states, the two barriers; the seat's activity mark and its dt
+// arrive while it computes its fluxes); a dense step spreads the queue over all
+// CTAs.
+//
+// Step control: the last CTA to arrive at a step's final barrier runs it for
+// every instance after the others have gone on, and publishes each instance's
+// next dt beside that step's epoch as one 64-bit pair (dt words 2..3), which
+// the next step's readers wait for (bounded) only where they need the dt.
 //
 // Activity: a block is active in step n if it was in the launch's start list
 // (n = 0) or a wet or forced block of its two-ring marked it with the step's
