@@ -488,9 +488,11 @@ def run_b200(args, world: int, rank: int, local: int) -> None:
         line["fp64_oracle_error"] = err
     del solver
     torch.cuda.empty_cache()
-    if not args.no_batch:
+    # the batched and forward+adjoint figures are single-GPU measurements: with N replicas the line reports the
+    # replicas' forward only
+    if not args.no_batch and world == 1:
         line["batched"] = run_batch(args, world, local)
-    if not args.no_adjoint:
+    if not args.no_adjoint and world == 1:
         line["adjoint"] = run_adjoint(args, world, local)
     if rank == 0:
         print(json.dumps(line), flush=True)
