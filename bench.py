@@ -479,8 +479,12 @@ def run_b200(args, world: int, rank: int, local: int) -> None:
             "max_abs_u_mps": float(max((np.abs(hu[wet]) / h[wet]).max(), (np.abs(hv[wet]) / h[wet]).max())),
             "volume_drift_rel": abs(solver.volume_fp64() - v0) / v0,
         }
-    if rank == 0 and not args.no_e2e:
-        line["e2e"] = e2e_run(solver, sc, t_sim, args)
+    if not args.no_e2e:  # every replica, over the slowest rank's wall time
+        e2e = e2e_run(solver, sc, t_sim, args)
+        if world > 1:
+            e2e["wall_s"] = reduce_max(e2e["wall_s"], world)
+            e2e["value"] = world * g.N * e2e["steps"] / e2e["wall_s"]
+        line["e2e"] = e2e
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         del graphs, warm
         cpu, err = cpu_baseline_and_error(sc, SWESolverB200Resident, device)
