@@ -345,6 +345,12 @@ int swe_eft_probe(float *v, swe_stream_t stream);
 int swe_open_ghost_probe(const float *cases, const uint32_t *cond, float *results, uint32_t n, float g,
                          float dry_tol, swe_stream_t stream);
 
+/* One bounded wait, on the device, for instance 0's published (dt, epoch) pair (dt words 2..3),
+   the wait the persistent kernel's seats make for the step control's dt: *out = the dt bits once
+   the pair carries `epoch`, or 0 after the 2 s limit, with error bit 4 set in instance 0's
+   control block. For tests of the limit: no counterpart in the reference. */
+int swe_dt_wait_probe(const swe_state_t *state, uint32_t epoch, uint32_t *out, swe_stream_t stream);
+
 /* (x^(4/3)) of n values on the device, the Manning depth power the update uses. */
 int swe_pow43(const float *x, float *out, uint32_t n, swe_stream_t stream);
 

@@ -75,6 +75,13 @@ __global__ void open_ghost_kernel(const float *cases, const uint32_t *cond, floa
     }
 }
 
+// One bounded wait for instance 0's published dt pair (the seats' wait in the
+// persistent kernel): the dt bits, or 0 and error bit 4 after the wait limit.
+__global__ void dt_wait_probe_kernel(swe_state_t s, uint32_t epoch, uint32_t *out) {
+    const uint64_t *pair = dt_pair(s, 0u);
+    out[0] = published_dt(s, pair, epoch, ld_relaxed_u64(pair));
+}
+
 }  // namespace swe
 
 using namespace swe;
@@ -95,6 +102,13 @@ int swe_volume_fp64(const float *h, const float *h_lo, const float *area, uint32
     int rc = check_launch();
     if (rc) return rc;
     volume_final_kernel<<<1, kThreads, 0, stream>>>(partials, parts, out);
+    return check_launch();
+}
+
+int swe_dt_wait_probe(const swe_state_t *state, uint32_t epoch, uint32_t *out, swe_stream_t stream) {
+    if (!state || !state->dt_buf || !state->ctrl || !out || (reinterpret_cast<uintptr_t>(state->dt_buf) & 15u))
+        return SWE_ERR_ARGUMENT;
+    dt_wait_probe_kernel<<<1, 1, 0, stream>>>(*state, epoch, out);
     return check_launch();
 }
 

@@ -124,3 +124,10 @@ def test_tile_layout_resolves_every_csr_slot(name: str) -> None:
             s0 = g.cell_edge_ptr[min(t * T.tile_cells, g.N)]
             s1 = g.cell_edge_ptr[min((t + 1) * T.tile_cells, g.N)]
             np.testing.assert_array_equal(T.lcsr_blk[T.lcsr_ptr[t]: T.lcsr_ptr[t] + s1 - s0], T.lcsr[s0:s1])
+
+
+def test_the_dt_wait_probe_refuses_a_misaligned_or_missing_buffer(lib: ctypes.CDLL) -> None:
+    state = native.SweState()
+    assert lib.swe_dt_wait_probe(ctypes.byref(state), 1, ctypes.c_void_p(16), None) == 1  # no dt words
+    state.dt_buf, state.ctrl = 0x20008, 0x30000
+    assert lib.swe_dt_wait_probe(ctypes.byref(state), 1, ctypes.c_void_p(16), None) == 1  # not 16-byte aligned
