@@ -274,6 +274,7 @@ class SWESolverB200Resident(ResidentEngine):
         wall0 = _time.monotonic()
         last_log = wall0
         finite = True
+        h_snap, snap_ticks = None, None  # the last window's depth and the clock it was read at
         for stop in output_window_stops(start_ticks, end_ticks, interval_ticks):
             ctrl["stop_ticks"] = stop
             self._sync_ctrl_to_device()
@@ -299,7 +300,7 @@ class SWESolverB200Resident(ResidentEngine):
                 if progress and now - last_log >= 10.0:
                     self._log_progress(now - wall0, now_ticks, start_ticks, end_ticks)
                     last_log = now
-            h_snap = self.download_h()
+            h_snap, snap_ticks = self.download_h(), int(ctrl["now_ticks"][0])
             if not np.isfinite(h_snap).all():
                 snapshots.append(np.nan_to_num(h_snap, nan=0.0, posinf=0.0))
                 snap_times.append(ticks_to_seconds(stop))
@@ -318,7 +319,9 @@ class SWESolverB200Resident(ResidentEngine):
                 capture()
         self.steps_total += int(ctrl["steps"][0])
         if finite:
-            h_final = self.download_h()
+            # the state has not moved since the last window's read when the clock has not
+            same = h_snap is not None and snap_ticks == int(ctrl["now_ticks"][0])
+            h_final = h_snap if same else self.download_h()
             if not (np.array_equal(snapshots[-1], h_final) or np.allclose(snapshots[-1], h_final)):
                 snapshots.append(h_final)
                 snap_times.append(ticks_to_seconds(int(ctrl["now_ticks"][0])))
