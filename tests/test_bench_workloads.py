@@ -1,8 +1,8 @@
 """The bench's workloads build at small sizes and describe themselves correctly (no GPU).
 
-``bench.py --workload W`` names the BASELINE-style configuration it measures in
-its JSON line's ``config``; these checks keep those descriptions tied to the
-scenarios actually built (cells, CFL, the L2 statement, the sources of the rain).
+``bench.py --workload W`` names the configuration it measures in its JSON line's
+``config``; these checks keep those descriptions tied to the scenarios actually
+built (cells, CFL, the L2 statement, the sources of the rain).
 """
 
 from __future__ import annotations
