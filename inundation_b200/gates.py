@@ -294,7 +294,7 @@ def dambreak(case: str = "stoker", nx: int = 500, ny: int = 5, t_end: float = 20
         travel = 2.0 * math.sqrt(GRAVITY_G * h_up) * t_end
         out["front_rel_err"] = abs((float(wet.max()) if wet.size else dam) - (dam + travel)) / travel
         gates["front_rel_err"] = 0.15
-    return _verdict(out, gates)
+    return _gate_result(out, gates)
 
 
 def radial(n: int = 200, t_end: float = 1.5) -> dict:
@@ -347,7 +347,7 @@ def radial(n: int = 200, t_end: float = 1.5) -> dict:
            "isotropy_spread": float((fronts_a.max() - fronts_a.min()) / fronts_a.mean()),
            "volume_drift_rel": abs(s.volume_fp64() - _volume(geom, h0.astype(np.float32))) / _volume(geom, h0),
            "min_depth_m": float(h.min()), "finite": bool(np.isfinite(h).all())}
-    return _verdict(out, {"l1_rel": 0.10, "front_rel_err": 0.05, "isotropy_spread": 0.08, "volume_drift_rel": 1e-5})
+    return _gate_result(out, {"l1_rel": 0.10, "front_rel_err": 0.05, "isotropy_spread": 0.08, "volume_drift_rel": 1e-5})
 
 
 def bowl(n: int = 200, periods: int = 3, cfl: float | None = None) -> dict:
@@ -381,7 +381,7 @@ def bowl(n: int = 200, periods: int = 3, cfl: float | None = None) -> dict:
     gates = {"film_speed_max_ms": 1.0, "volume_drift_rel": 1e-7, "clamp_rel": 0.0}
     if n == 200:
         gates["depth_l1_rel_mean"] = 0.18
-    return _verdict(out, gates, strict=("depth_l1_rel_mean", "film_speed_max_ms", "volume_drift_rel"))
+    return _gate_result(out, gates, strict=("depth_l1_rel_mean", "film_speed_max_ms", "volume_drift_rel"))
 
 
 def lake(cells: int = 8000, t_end: float = 600.0) -> dict:
@@ -399,7 +399,7 @@ def lake(cells: int = 8000, t_end: float = 600.0) -> dict:
     max_u = float(max((np.abs(hu[wet]) / h[wet]).max(), (np.abs(hv[wet]) / h[wet]).max()))
     out = {"case": "lake", "cells": sc.geom.N, "steps": s.steps_total, "wall_s": wall, "max_speed_ms": max_u,
            "volume_drift_rel": abs(s.volume_fp64() - v0) / v0}
-    return _verdict(out, {"max_speed_ms": 0.01, "volume_drift_rel": 1e-9})
+    return _gate_result(out, {"max_speed_ms": 0.01, "volume_drift_rel": 1e-9})
 
 
 def uniform(cells: int = 200, length: float = 2000.0, width: float = 40.0, across: int = 2,
@@ -432,7 +432,7 @@ def uniform(cells: int = 200, length: float = 2000.0, width: float = 40.0, acros
            "depth_error_rel": abs(float(h[middle].mean()) / hn - 1.0),
            "discharge_error_rel": abs((went_out[-1] - went_out[-2]) / (t_end / 8.0) / discharge - 1.0),
            "inflow_error_rel": abs(s.download_open_volumes()[0, 1] / (discharge * t_end) - 1.0)}
-    return _verdict(out, {"depth_error_rel": 0.01, "discharge_error_rel": 1e-3, "inflow_error_rel": 1e-7},
+    return _gate_result(out, {"depth_error_rel": 0.01, "discharge_error_rel": 1e-3, "inflow_error_rel": 1e-7},
                     strict=("depth_error_rel", "discharge_error_rel", "inflow_error_rel"))
 
 
@@ -460,7 +460,7 @@ def held_lake(cells: int = 200, length: float = 1000.0, width: float = 40.0, acr
     speed = float(np.hypot(s.download_hu(), s.download_hv()).max() / h.min())
     out = {"case": "held_lake", "cells": geom.N, "steps": s.steps_total, "wall_s": wall,
            "level_error_m": float(np.abs(h + zb - level).max()), "speed_max_ms": speed}
-    return _verdict(out, {"level_error_m": 1e-4, "speed_max_ms": 1e-3}, strict=("level_error_m", "speed_max_ms"))
+    return _gate_result(out, {"level_error_m": 1e-4, "speed_max_ms": 1e-3}, strict=("level_error_m", "speed_max_ms"))
 
 
 def _workflow(geom: MeshGeometry, ends: list, *, output_interval_s: float, manning: float = 0.03):
@@ -510,7 +510,7 @@ def backwater(end_depth: float = 0.8, cells: int = 600, length: float = 3000.0, 
            "profile_error_rel": float((np.abs(h - ref) / ref)[1:-1].max()),
            "discharge_error_rel": abs((went_out[-1] - went_out[-2]) / window / discharge - 1.0),
            "balance_rel": _balance_rel(r)}
-    return _verdict(out, {"profile_error_rel": 0.015, "discharge_error_rel": 1e-3, "balance_rel": 1e-7},
+    return _gate_result(out, {"profile_error_rel": 0.015, "discharge_error_rel": 1e-3, "balance_rel": 1e-7},
                     strict=("profile_error_rel", "discharge_error_rel", "balance_rel"))
 
 
@@ -557,10 +557,10 @@ def basins(cells: int = 400, length: float = 4000.0, width: float = 40.0, slope:
            "upper_balance_rel": _balance_rel(first), "balance_rel": _balance_rel(second)}
     gates = {"passed_error_rel": 1e-6, "depth_difference_rel": 0.01, "outflow_difference_rel": 0.02,
              "upper_balance_rel": 1e-7, "balance_rel": 1e-7}
-    return _verdict(out, gates, strict=tuple(gates))
+    return _gate_result(out, gates, strict=tuple(gates))
 
 
-def _verdict(out: dict, gates: dict, strict: tuple[str, ...] = ()) -> dict:
+def _gate_result(out: dict, gates: dict, strict: tuple[str, ...] = ()) -> dict:
     """``passed`` and the failed gates: a value above its gate fails (at or above for ``strict``)."""
     failed = []
     for key, bound in gates.items():
