@@ -69,10 +69,12 @@ def test_repeat_runs_are_bit_identical(case: str, grid) -> None:
     assert_identical(a, b, run(a, t_end, source_rate=src), run(b, t_end, source_rate=src))
 
 
-def test_stale_predictor_state_is_never_read(grid) -> None:
+@pytest.mark.parametrize("kernel", ["tiled", "plain", "persistent"])
+@pytest.mark.parametrize("fill", [0.5, float("nan")], ids=["wet", "nan"])
+def test_stale_predictor_state_is_never_read(kernel: str, fill: float, grid) -> None:
     h0 = dam(grid)
-    clean, poisoned = make(grid, h0), make(grid, h0)
-    garbage = np.full(grid.N, 0.5, np.float32)
+    clean, poisoned = make(grid, h0, stage_kernel=kernel), make(grid, h0, stage_kernel=kernel)
+    garbage = np.full(grid.N, fill, np.float32)  # wet garbage, or NaN that any read would carry into the state
     for name in ("h1", "hu1", "hv1"):
         poisoned.upload(name, garbage)
     assert_identical(clean, poisoned, run(clean, 30.0), run(poisoned, 30.0))
