@@ -244,7 +244,8 @@ class SWESolverB200Resident(ResidentEngine):
         if not resume:
             self._reset_to_initial()
             self.open_volume_snapshots = []
-        if self.compensated:
+        # The open-edge volume tally is a two-sum too (gpu_resident_batch.py:659-660).
+        if self.compensated or self.n_open:
             self._check_error_free_arithmetic()
         self._set_sources(source_rate)
 

@@ -56,6 +56,24 @@ def _i32(a: NDArray) -> NDArray[np.int32]:
     return np.ascontiguousarray(a).view(np.int32)
 
 
+# The two-sum probe's input: its third word comes back as the error term of 1 + 1e-9.
+EFT_PROBE_WORDS = (1.0, 1e-9, 0.0)
+
+
+def check_eft_probe(words: NDArray[np.float32]) -> None:
+    """Raise if the probe lost two-sum's error term, which must be 1e-9 exactly in float32.
+
+    The reference refuses to run then (``inundation/vulkan/solver.py:461-466``):
+    compensated depth and the open-edge tallies would leak mass.
+    """
+    got = np.asarray(words, np.float32).ravel()
+    if got.size != 3 or float(got[2]) != float(np.float32(EFT_PROBE_WORDS[1])):
+        raise RuntimeError(
+            "error-free arithmetic is broken on this device, so compensated depth would leak mass: "
+            "rebuild the library without fast math, or set compensated = False"
+        )
+
+
 class ResidentEngine:
     """Device buffers and kernel launches of a batch of meshes (a single mesh is a batch of one)."""
 
@@ -393,15 +411,18 @@ class ResidentEngine:
         return int(self._sched.cpu().numpy().view(np.uint64)[3])
 
     # -- kernels ----------------------------------------------------------------------------------
-    def _check_error_free_arithmetic(self) -> None:
-        if self._eft_checked:
-            return
-        v = torch.tensor([1.0, 1e-9, 0.0], dtype=torch.float32, device=self.device)
+    def _eft_probe(self) -> NDArray[np.float32]:
+        """The device's two-sum of 1 and 1e-9: words (1, 1e-9, error term)."""
+        v = torch.tensor(EFT_PROBE_WORDS, dtype=torch.float32, device=self.device)
         with torch.cuda.stream(self._stream):
             native.check(self._lib.swe_eft_probe(v.data_ptr(), self._cuda_stream), "swe_eft_probe")
-            got = v.cpu().numpy()
-        if float(got[2]) != float(np.float32(1e-9)):
-            raise RuntimeError("error-free arithmetic is broken on this device, so compensated depth would leak mass")
+            return v.cpu().numpy()
+
+    def _check_error_free_arithmetic(self) -> None:
+        """Refuse to run once if the device loses two-sum's error term (solver.py:449-467)."""
+        if self._eft_checked:
+            return
+        check_eft_probe(self._eft_probe())
         self._eft_checked = True
 
     def _sync_ctrl_to_device(self) -> None:

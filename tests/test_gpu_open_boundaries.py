@@ -188,3 +188,21 @@ def test_repeat_runs_are_bit_identical() -> None:
     b, _ = run(s, t_end)
     np.testing.assert_array_equal(bits(a[-1]), bits(b[-1]))
     np.testing.assert_array_equal(va, s.download_open_volumes())
+
+
+def test_an_open_mesh_checks_the_two_sum_even_uncompensated(monkeypatch) -> None:
+    """The open-edge tallies are two-sums: the guard runs for an open mesh with compensated off
+    (the reference's ``compensated or n_open``, gpu_resident_batch.py:659-660)."""
+    sc, kinds, values, t_end = channel("draining")
+    s = solver_of(sc, kinds, values)
+    s.compensated = False
+    probes = []
+
+    def lost():
+        probes.append(1)
+        return np.array([1.0, 1e-9, 0.0], np.float32)
+
+    monkeypatch.setattr(s, "_eft_probe", lost)
+    with pytest.raises(RuntimeError, match="error-free arithmetic is broken"):
+        run(s, 1.0)
+    assert probes and s.steps_total == 0

@@ -366,7 +366,8 @@ def test_adaptive_run_with_sources_matches_the_fp32_oracle(kernel: str) -> None:
 
 # -- workflow ------------------------------------------------------------------------------------------------
 def test_workflow_runs_phases_end_to_end() -> None:
-    from inundation_b200.workflow import PointSource, SimulationPhase, SWEWorkflow, WorkflowConfig
+    """Two phases through the public API, bit for bit against the FP32 oracle run through the same phases."""
+    from inundation_b200.workflow import PointSource, SimulationPhase, SWEWorkflow, WorkflowConfig, build_phase_source_rate
 
     g = valley_grid(nx=64, ny=32)
     cfg = WorkflowConfig(mesh_source=None, geometry_cache_source="unused.npz", manning_n=MANNING, output_interval_s=20.0,
@@ -379,7 +380,82 @@ def test_workflow_runs_phases_end_to_end() -> None:
               SimulationPhase(30.0, [PointSource(1.0, (x0 + 40.0, y0 + 32.0), 3.0)])]
     res = wf.run(phases)
     assert res.volume_injected_m3 == pytest.approx(45.0)
-    assert res.volume_final_m3 == pytest.approx(45.0 - (res.clamp_mass_m3 or 0.0) * 0.0, rel=1e-4)
+    # positivity clamps add their mass to what the sources put in (reference workflow.py:913-945)
+    assert res.clamp_mass_m3 is not None and res.clamp_mass_m3 >= 0.0
+    assert res.volume_final_m3 == pytest.approx(res.volume_injected_m3 + res.clamp_mass_m3, rel=1e-6)
     assert res.snap_times[0] == 0.0 and res.snap_times[-1] == 60.0
     assert len(res.hu_snapshots) == len(res.snapshots) == len(res.snap_times)
     assert res.steps_total > 0 and res.h_final.shape == (g.N,)
+
+    # the same phases on the FP32 oracle: every snapshot and the final state bit for bit
+    geom = wf.geom
+    zero = np.zeros(geom.N, np.float32)
+    oracle = ResidentOracle(geom, wf.solver._h0, zero, zero, np.full(geom.N, MANNING, np.float32), dry_tol=DRY_TOL,
+                            steps_per_graph=wf.solver.steps_per_graph)
+    oracle.track_clamp = True
+    valid = geom.area > cfg.area_tol
+    snaps, times, t = [], [], 0.0
+    for k, phase in enumerate(phases):
+        s, ts = oracle.run(t_end=t + phase.duration_s, output_interval_s=cfg.output_interval_s, dt_max=cfg.dt_max,
+                           dt_init=cfg.dt_init, source_rate=build_phase_source_rate(geom, phase, valid),
+                           resume=k > 0, t_start=t)
+        snaps += s
+        times += ts
+        t += phase.duration_s
+    assert res.steps_total == oracle.steps_total
+    assert res.snap_times == times
+    for a, b in zip(res.snapshots, snaps, strict=True):
+        np.testing.assert_array_equal(bits(a), bits(b))
+    for a, b in ((res.h_final, oracle.download_h()), (res.hu_final, oracle.download_hu()),
+                 (res.hv_final, oracle.download_hv()), (wf.solver.download_h_residual(), oracle.download_h_residual()),
+                 (wf.solver.download_clamp_mass(), oracle.download_clamp_mass())):
+        np.testing.assert_array_equal(bits(a), bits(b))
+
+
+# -- the run loop's failure branches (reference gpu_resident_batch.py:715-736) --------------------------------
+def test_a_bound_below_one_tick_stops_the_run_with_no_progress(grid) -> None:
+    """A CFL bound under 2^-20 s rounds to zero ticks: the run raises instead of stalling."""
+    h0 = np.ones(grid.N, np.float32)
+    hu0 = np.zeros(grid.N, np.float32)
+    hu0[grid.N // 2] = 1e9  # a velocity of 1e9 m/s on 2 m cells: a bound of ~1e-9 s
+    solver = make(grid, h0, hu0)
+    with pytest.raises(RuntimeError, match=r"made no time progress at t=0\.000000s \(CFL bound below one tick\)"):
+        run(solver, 1.0)
+    oracle = ResidentOracle(grid, h0, hu0, np.zeros(grid.N, np.float32), np.full(grid.N, MANNING, np.float32))
+    with pytest.raises(RuntimeError, match="no time progress"):
+        oracle.run(t_end=1.0, output_interval_s=0.25, dt_max=1.0, dt_init=0.01)
+
+
+def test_a_non_finite_depth_ends_the_run_with_a_cleaned_snapshot(grid) -> None:
+    """NaN in the state: the window's snapshot is nan_to_num'd, it is the last one, and run() returns."""
+    h0 = dam(grid)
+    h0[0] = np.nan
+    solver = make(grid, h0)
+    snaps, times = solver.run(t_end=40.0, output_interval_s=10.0, dt_max=1.0, dt_init=0.01, cfl_interval=1,
+                              progress=False)
+    assert times == [0.0, 10.0]  # stopped after the first window
+    assert len(snaps) == 2 and np.isnan(snaps[0][0])  # the initial state as given
+    assert np.isfinite(snaps[1]).all()
+    h_dev = solver.download_h()
+    assert not np.isfinite(h_dev).all()
+    bad = ~np.isfinite(h_dev)
+    assert (snaps[1][bad] == 0.0).all()
+    np.testing.assert_array_equal(bits(snaps[1][~bad]), bits(h_dev[~bad]))
+    assert 0 < solver.steps_total
+    oracle = ResidentOracle(grid, h0, np.zeros(grid.N, np.float32), np.zeros(grid.N, np.float32),
+                            np.full(grid.N, MANNING, np.float32))
+    o_snaps, o_times = oracle.run(t_end=40.0, output_interval_s=10.0, dt_max=1.0, dt_init=0.01)
+    assert o_times == times and oracle.steps_total == solver.steps_total
+    np.testing.assert_array_equal(bits(o_snaps[1]), bits(snaps[1]))
+
+
+def test_a_device_that_loses_the_two_sum_error_is_refused(grid, monkeypatch) -> None:
+    """The guard's refusing branch: a probe whose error term comes back lost stops run() before any step."""
+    solver = make(grid, dam(grid))
+    monkeypatch.setattr(solver, "_eft_probe", lambda: np.array([1.0, 1e-9, 0.0], np.float32))
+    with pytest.raises(RuntimeError, match="error-free arithmetic is broken"):
+        run(solver, 1.0)
+    assert solver.steps_total == 0
+    solver.compensated = False  # a closed mesh without the compensated pair needs no check
+    run(solver, 1.0)
+    assert solver.steps_total > 0

@@ -4,6 +4,7 @@ The rule: the persistent whole-step kernel while at most a quarter of the blocks
 are active, or while every active 64-cell tile has a CTA of its grid to itself
 (a small mesh); the 256-cell block kernel otherwise, and always when the
 persistent grid cannot hold a step (one seat and 512 other tiles per CTA).
+Also the two-sum guard's verdict on a probe's words.
 """
 
 from __future__ import annotations
@@ -62,3 +63,15 @@ def test_explicit_choice_and_unknown_names() -> None:
     e.stage_kernel = "fastest"
     with pytest.raises(ValueError, match="stage_kernel"):
         _ = e._kernel
+
+
+def test_two_sum_probe_verdicts() -> None:
+    """The guard's decision on the probe's words (the device half runs in the GPU tests)."""
+    import numpy as np
+
+    from inundation_b200.engine import check_eft_probe
+
+    check_eft_probe(np.array([1.0, 1e-9, 1e-9], np.float32))  # the exact error term: accepted
+    for words in ([1.0, 1e-9, 0.0], [1.0, 1e-9, np.nan], [1.0, 1e-9, 2e-9], [1.0, 1e-9]):
+        with pytest.raises(RuntimeError, match="error-free arithmetic is broken"):
+            check_eft_probe(np.array(words, np.float32))
