@@ -86,6 +86,14 @@ def parse_args() -> argparse.Namespace:
     ap.add_argument("--adjoint-steps", type=int, default=2000)
     ap.add_argument("--spin-up", type=float, default=60.0,
                     help="rain_inflow: simulated seconds run before the timed steps")
+    ap.add_argument("--no-hour", action="store_true", help="skip the whole simulated hour of the dam break")
+    ap.add_argument("--no-horizon", action="store_true", help="skip the float64 error at 8, 64 and 512 steps")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the lake-at-rest and rain-plus-inflow configurations of the default line")
+    ap.add_argument("--adjoint-fd", action="store_true",
+                    help="only check the adjoint at 250k cells against float64 central differences and print that")
+    ap.add_argument("--fd-steps", type=int, default=200, help="--adjoint-fd: steps of the checked run")
+    ap.add_argument("--fd-directions", type=int, default=20, help="--adjoint-fd: random directions")
     args = ap.parse_args()
     cells, seed = WORKLOADS[args.workload]
     args.cells = cells if args.cells is None else args.cells
@@ -343,6 +351,8 @@ def cpu_baseline_and_error(sc, solver_cls, device: str) -> tuple[dict, dict]:
         "unit": UNIT,
         "cores": 1,
         "kind": "port",
+        "source": "oracle/fp64_step.py: the reference's float64 CPU step tests/unit/_cpu_step.py restated, "
+        "pinned to that file's outputs to 1e-12 by tests/golden/cpu_step.npz",
         "sample": f"{timed} float64 Heun steps (dt={dt:g} s) of the full {g.N}-cell mesh, single process, "
         f"{wall:.1f} s",
     }
@@ -357,25 +367,22 @@ def cpu_baseline_and_error(sc, solver_cls, device: str) -> tuple[dict, dict]:
     return cpu, err
 
 
-def run_b200(args, world: int, rank: int, local: int) -> None:
+def forward_line(args, sc, world: int, local: int):
+    """Exactly ``args.steps`` steps of ``sc`` after ``args.warmup``, timed on the device: the line's
+    measured keys, and the solver with the simulated seconds of the timed steps."""
     import torch
 
     from inundation_b200.backend import SWESolverB200Resident
     from inundation_b200.layout import algorithmic_bytes_per_cell_step
 
     device = f"cuda:{local}"
-    torch.cuda.set_device(local)
-    if args.workload == "rain_inflow":
-        run_sources_workload(args, world, rank, local)
-        return
-    sc = build_scenario(args.workload, args.cells, args.seed)
     g = sc.geom
     cfl = float(sc.meta.get("cfl", 0.8))
     solver = SWESolverB200Resident(g, None, sc.h0, sc.hu0, sc.hv0, sc.manning, dry_tol=sc.dry_tol, cfl=cfl,
                                    device=device)
     solver.stage_kernel = args.kernel
     solver.ctas_per_sm = args.ctas_per_sm
-    v0 = solver.volume_fp64() if args.workload == "lake_at_rest" else None
+    v0 = solver.volume_fp64() if sc.name == "lake_at_rest" else None
     plan(solver, sc)
     if args.kernel == "auto":  # the choice "auto" makes for this state, fixed for the timed region
         from inundation_b200.engine import KERNELS
@@ -479,27 +486,298 @@ def run_b200(args, world: int, rank: int, local: int) -> None:
             "max_abs_u_mps": float(max((np.abs(hu[wet]) / h[wet]).max(), (np.abs(hv[wet]) / h[wet]).max())),
             "volume_drift_rel": abs(solver.volume_fp64() - v0) / v0,
         }
+    del graphs, warm
+    return line, solver, t_sim
+
+
+def run_b200(args, world: int, rank: int, local: int) -> None:
+    import torch
+
+    from inundation_b200.backend import SWESolverB200Resident
+
+    device = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    if args.workload == "rain_inflow":
+        line = run_sources_workload(args, world, rank, local)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        return
+    # The default line (the 1M-cell dam break on one GPU) also carries the other configurations;
+    # the meshes of the 4M-cell one and the float64 error's oracle run in other processes meanwhile.
+    full = args.workload == "dam_break" and world == 1 and not args.no_configs
+    helpers = None
+    if full or (args.workload == "dam_break" and world == 1 and not args.no_horizon):
+        import concurrent.futures as cf
+        import multiprocessing as mp
+
+        helpers = cf.ProcessPoolExecutor(max_workers=2, mp_context=mp.get_context("spawn"))
+    rain_future = helpers.submit(_build_timed, "rain_inflow", WORKLOADS["rain_inflow"][0],
+                                 WORKLOADS["rain_inflow"][1]) if full else None
+    sc = build_scenario(args.workload, args.cells, args.seed)
+    line, solver, t_sim = forward_line(args, sc, world, local)
+    g = sc.geom
     if not args.no_e2e:  # every replica, over the slowest rank's wall time
         e2e = e2e_run(solver, sc, t_sim, args)
         if world > 1:
             e2e["wall_s"] = reduce_max(e2e["wall_s"], world)
             e2e["value"] = world * g.N * e2e["steps"] / e2e["wall_s"]
         line["e2e"] = e2e
+    del solver
+    torch.cuda.empty_cache()
+    horizon_job = None
+    if helpers is not None and not args.no_horizon:
+        horizon_job = start_error_by_horizon(sc, device, helpers)
     if rank == 0 and not args.no_cpu_baseline and world == 1:
-        del graphs, warm
         cpu, err = cpu_baseline_and_error(sc, SWESolverB200Resident, device)
         line["cpu_baseline"] = cpu
         line["fp64_oracle_error"] = err
-    del solver
-    torch.cuda.empty_cache()
-    # the batched and forward+adjoint figures are single-GPU measurements: with N replicas the line reports the
-    # replicas' forward only
+    # the whole-run, batched, forward+adjoint and other-configuration figures are single-GPU
+    # measurements: with N replicas the line reports the replicas' forward only
+    if args.workload == "dam_break" and world == 1 and not args.no_hour:
+        line["whole_run"] = run_whole_hour(sc, args, device)
     if not args.no_batch and world == 1:
         line["batched"] = run_batch(args, world, local)
     if not args.no_adjoint and world == 1:
         line["adjoint"] = run_adjoint(args, world, local)
+    if full:
+        line["configs"] = {
+            "lake_at_rest": config_lake_at_rest(args, world, local),
+            "rain_inflow": config_rain_inflow(args, world, rank, local, rain_future.result()),
+        }
+    if horizon_job is not None:
+        line["fp64_error_by_horizon"] = finish_error_by_horizon(*horizon_job)
+    if helpers is not None:
+        helpers.shutdown()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def sub_args(args, **overrides) -> argparse.Namespace:
+    """A copy of the command line for another configuration of the same run."""
+    return argparse.Namespace(**{**vars(args), **overrides})
+
+
+def _build_timed(name: str, cells: int, seed: int):
+    """A scenario and the seconds its build took (run in a helper process)."""
+    os.environ.setdefault("OMP_NUM_THREADS", "4")
+    t0 = time.perf_counter()
+    sc = build_scenario(name, cells, seed)
+    return sc, time.perf_counter() - t0
+
+
+def config_lake_at_rest(args, world: int, local: int) -> dict:
+    """Configuration 1: ~8k cells over 1 km, six Gaussian bumps under a still 1 m surface, CFL 0.9,
+    2000 timed steps (after the warm-up), then the reference's lake gate (max |u| over cells deeper
+    than 10 dry_tol) and the float64 volume drift."""
+    import torch
+
+    cells, seed = WORKLOADS["lake_at_rest"]
+    a = sub_args(args, workload="lake_at_rest", cells=cells, seed=seed, steps=2000, kernel="auto")
+    sc = build_scenario("lake_at_rest", cells, seed)
+    line, solver, t_sim = forward_line(a, sc, world, local)
+    line["e2e"] = e2e_run(solver, sc, t_sim, a)
+    del solver
+    torch.cuda.empty_cache()
+    keep = ("value", "ms_per_step", "steps", "warmup", "computed_cell_steps_per_s", "active_fraction",
+            "simulated_s", "gpu_launches", "roofline", "lake_at_rest_check", "e2e", "config", "clocks")
+    return {k: line[k] for k in keep if k in line}
+
+
+def config_rain_inflow(args, world: int, rank: int, local: int, built) -> dict:
+    """Configuration 3: 4M cells over 20 km, 40 m relief, rain 50 mm/h on every cell plus a
+    triangular 200 m^3/s inflow, timed over 200 steps after the ``--spin-up`` seconds in which
+    the rain wets the mesh (the mesh was built in a helper process meanwhile)."""
+    cells, seed = WORKLOADS["rain_inflow"]
+    a = sub_args(args, workload="rain_inflow", cells=cells, seed=seed, steps=max(args.steps, 200), kernel="auto")
+    line = run_sources_workload(a, world, rank, local, built=built)
+    drop = ("metric", "unit", "n_gpus", "higher_is_better", "scaling", "vs_baseline", "dtype", "data")
+    return {k: v for k, v in line.items() if k not in drop}
+
+
+def run_whole_hour(sc, args, device: str) -> dict:
+    """Configuration 2 as it is defined: the dam break over one simulated hour through ``run()``
+    (output every 5 min, the kernel picked by ``stage_kernel = "auto"`` after every submit).
+
+    The reference's whole-run convention: cells x steps over the run's wall time
+    (``inundation/bench/flood_propagation.py:646``). The trajectory gives, per output
+    window, the steps, the wall time, the computed (active) fraction and the steps
+    each kernel ran; the switches list when "auto" changed kernel.
+    """
+    import torch
+
+    from inundation_b200.backend import SWESolverB200Resident
+    from inundation_b200.tuning import SIM_TICKS_PER_SECOND
+
+    g = sc.geom
+    t_end, interval = 3600.0, 300.0
+    solver = SWESolverB200Resident(g, None, sc.h0, sc.hu0, sc.hv0, sc.manning, dry_tol=sc.dry_tol, cfl=0.8,
+                                   device=device)
+    solver.steps_per_graph = 500
+    solver.run(t_end=1.0, output_interval_s=1.0, dt_max=sc.dt_max, dt_init=sc.dt_init, cfl_interval=1,
+               progress=False)  # the two-sum probe and the first kernel's set-up, outside the timing
+    solver.submit_log = log = []
+    computed0 = solver.computed_cells
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    t0 = time.perf_counter()
+    w0 = time.monotonic()
+    snaps, times = solver.run(t_end=t_end, output_interval_s=interval, dt_max=sc.dt_max, dt_init=sc.dt_init,
+                              cfl_interval=1, progress=False)
+    wall = time.perf_counter() - t0
+    clock = clocks.stop()
+    steps = sum(r.steps for r in log)
+    computed = log[-1].computed_cells - computed0 if log else 0
+    per_tick = float(SIM_TICKS_PER_SECOND)
+    windows = []
+    prev_wall, prev_computed = w0, computed0
+    for k in range(int(round(t_end / interval))):
+        lo, hi = k * interval * per_tick, (k + 1) * interval * per_tick
+        recs = [r for r in log if lo < r.now_ticks <= hi]
+        if not recs:
+            continue
+        n = sum(r.steps for r in recs)
+        kernels: dict[str, int] = {}
+        for r in recs:
+            kernels[r.kernel] = kernels.get(r.kernel, 0) + r.steps
+        c = recs[-1].computed_cells - prev_computed
+        windows.append({
+            "t_end_s": (k + 1) * interval,
+            "steps": n,
+            "wall_s": recs[-1].wall_s - prev_wall,
+            "active_fraction": c / (g.N * n) if n else 0.0,
+            "active_blocks_at_end": recs[-1].active_blocks / solver.n_blocks,
+            "kernel_steps": kernels,
+        })
+        prev_wall, prev_computed = recs[-1].wall_s, recs[-1].computed_cells
+    switches = []
+    for a, b in zip(log[:-1], log[1:]):
+        if a.kernel != b.kernel:
+            switches.append({"t_s": a.now_ticks / per_tick, "from": a.kernel, "to": b.kernel,
+                             "active_blocks": a.active_blocks / solver.n_blocks})
+    volume = solver.volume_fp64()
+    del solver
+    torch.cuda.empty_cache()
+    return {
+        "workload": f"dam_break_{g.N // 1000}k_voronoi, one simulated hour",
+        "simulated_s": t_end,
+        "output_interval_s": interval,
+        "steps": steps,
+        "wall_s": wall,
+        "value": g.N * steps / wall,
+        "unit": UNIT,
+        "ms_per_step": wall * 1e3 / steps,
+        "computed_cell_steps_per_s": computed / wall,
+        "mean_active_fraction": computed / (g.N * steps),
+        "snapshots": len(snaps),
+        "volume_final_m3": volume,
+        "volume_initial_m3": float((sc.h0.astype(np.float64) * g.area.astype(np.float64)).sum()),
+        "trajectory": windows,
+        "kernel_switches": switches,
+        "clocks": clock,
+        "note": "host wall time of SWESolverB200Resident.run(t_end=3600) with the state resident: control-block "
+        "reads after every 500-step submit and the 12 snapshot downloads included (the reference's whole-run "
+        "convention)",
+    }
+
+
+# -- float64 error by horizon ---------------------------------------------------------------------
+HORIZONS = (8, 64, 512)
+
+
+def _fp64_region_run(region, h0, hu0, hv0, n, dts, horizons, dry_tol: float) -> dict:
+    """The float64 oracle over a region of the mesh with a given dt per step (run in a helper process):
+    the state at every horizon, and the deepest water on the region's rim by then."""
+    sys.path.insert(0, str(ROOT))
+    from oracle import fp64_step
+
+    s = fp64_step.State(np.asarray(h0, np.float64), np.asarray(hu0, np.float64), np.asarray(hv0, np.float64))
+    n64 = np.asarray(n, np.float64)
+    out, rim = {}, 0.0
+    t0 = time.perf_counter()
+    for k, dt in enumerate(dts, start=1):
+        s = fp64_step.heun_step(region, s, n64, float(dt), g=9.81, dry_tol=dry_tol)
+        rim = max(rim, float(s.h[region.rim].max()) if region.rim.size else 0.0)
+        if k in horizons:
+            out[k] = (s.h.copy(), s.hu.copy(), s.hv.copy(), rim)
+    return {"states": out, "cpu_s": time.perf_counter() - t0}
+
+
+def start_error_by_horizon(sc, device: str, pool, horizons=HORIZONS):
+    """The CUDA run of the dam break for max(horizons) adaptive steps, one step per submit (each step's
+    dt read from the control block), and the float64 oracle's run with those dt in a helper process.
+
+    The oracle runs over the region the water can reach by the last horizon (every cell within the
+    dam's radius plus 25 m/s times the simulated time plus 100 m); cells outside it stay dry in
+    both runs, which the result checks: the region's rim must stay dry in the oracle, every cell
+    outside it in the CUDA run.
+    """
+    import torch
+
+    from oracle import fp64_step
+    from inundation_b200.backend import SWESolverB200Resident
+
+    g = sc.geom
+    solver = SWESolverB200Resident(g, None, sc.h0, sc.hu0, sc.hv0, sc.manning, dry_tol=sc.dry_tol, cfl=0.8,
+                                   device=device)
+    plan(solver, sc)
+    before = int(solver._ctrl["now_ticks"][0])
+    dts, states = [], {}
+    for k in range(1, max(horizons) + 1):
+        sub = solver._graph(1)  # "auto" may change kernel between steps; every kernel gives the same bits
+        with torch.cuda.stream(solver._stream):
+            sub.replay()
+        solver._read_ctrl()
+        now = int(solver._ctrl["now_ticks"][0])
+        if now == before:
+            raise RuntimeError("the error-by-horizon run made no progress")
+        dts.append((now - before) / 2**20)
+        before = now
+        if k in horizons:
+            states[k] = (solver.download_h_precise(), solver.download_hu().astype(np.float64),
+                         solver.download_hv().astype(np.float64))
+    del solver
+    torch.cuda.empty_cache()
+    xy = g.world_centroid
+    centre = np.asarray(sc.meta["centre_m"], np.float64)
+    reach = float(sc.meta["radius_m"]) + 25.0 * float(sum(dts)) + 100.0
+    cells = np.flatnonzero(np.hypot(xy[:, 0] - centre[0], xy[:, 1] - centre[1]) <= reach)
+    region = fp64_step.restrict(g, cells)
+    fut = pool.submit(_fp64_region_run, region, sc.h0[cells], sc.hu0[cells], sc.hv0[cells], sc.manning[cells],
+                      dts, tuple(horizons), sc.dry_tol)
+    return fut, region, states, dts, reach
+
+
+def finish_error_by_horizon(fut, region, states, dts, reach) -> dict:
+    got = fut.result()
+    outside = np.ones(states[max(states)][0].size, bool)
+    outside[region.cells] = False
+    rows = []
+    for k, (h, hu, hv) in sorted(states.items()):
+        h64, hu64, hv64, rim = got["states"][k]
+        rows.append({
+            "steps": k,
+            "simulated_s": float(sum(dts[:k])),
+            "h_max_abs_m": float(np.abs(h[region.cells] - h64).max()),
+            "hu_max_abs": float(np.abs(hu[region.cells] - hu64).max()),
+            "hv_max_abs": float(np.abs(hv[region.cells] - hv64).max()),
+            "h_rms_wet_m": float(np.sqrt(np.mean((h[region.cells] - h64)[h64 > 0] ** 2))) if (h64 > 0).any() else 0.0,
+            "wet_cells": int((h64 > 0).sum()),
+            "oracle_rim_max_h_m": rim,
+            "cuda_max_h_outside_m": float(np.abs(h[outside]).max()) if outside.any() else 0.0,
+        })
+    held = all(r["oracle_rim_max_h_m"] == 0.0 and r["cuda_max_h_outside_m"] == 0.0 for r in rows)
+    return {
+        "protocol": "CUDA float32 run of the dam break with its own adaptive dt; the float64 oracle "
+        "(oracle/fp64_step.py, the reference's _cpu_step restated) from the same float32 initial state "
+        "with the same dt per step; depth is h + h_lo",
+        "mesh_cells": int(states[max(states)][0].size),
+        "oracle_region_cells": int(region.N),
+        "oracle_region_radius_m": reach,
+        "region_held": held,  # no water reached the oracle region's rim, none left it in the CUDA run
+        "oracle_cpu_s": got["cpu_s"],
+        "tolerance_h_m": 1e-5,
+        "horizons": rows,
+    }
 
 
 def e2e_run(solver, sc, t_sim: float, args) -> dict:
@@ -532,13 +810,14 @@ def e2e_run(solver, sc, t_sim: float, args) -> dict:
     }
 
 
-def run_sources_workload(args, world: int, rank: int, local: int) -> None:
+def run_sources_workload(args, world: int, rank: int, local: int, built=None) -> dict:
     """Rain on every cell plus an inflow hydrograph: the sparse-sources path, timed after a spin-up.
 
     One ``BatchedSolver`` instance (the solver that takes hydrographs). The mesh
     starts dry; the timed steps begin once ``--spin-up`` simulated seconds have
     run, by when the rain has wetted it. The end-to-end run uploads that state
     from host arrays, restarts the clock and runs the same number of steps.
+    ``built``: the scenario and its build seconds, when built beforehand.
     """
     import torch
 
@@ -547,9 +826,12 @@ def run_sources_workload(args, world: int, rank: int, local: int) -> None:
     from inundation_b200.layout import algorithmic_bytes_per_cell_step
 
     device = f"cuda:{local}"
-    t_build = time.perf_counter()
-    sc = build_scenario(args.workload, args.cells, args.seed)
-    t_build = time.perf_counter() - t_build
+    if built is None:
+        t_build = time.perf_counter()
+        sc = build_scenario(args.workload, args.cells, args.seed)
+        t_build = time.perf_counter() - t_build
+    else:
+        sc, t_build = built
     g = sc.geom
     member = BatchMember(g, sc.h0, sc.hu0, sc.hv0, sc.manning, source_rate=sc.source_rate,
                          hydrographs=sc.hydrographs)
@@ -659,8 +941,7 @@ def run_sources_workload(args, world: int, rank: int, local: int) -> None:
     }
     del solver
     torch.cuda.empty_cache()
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    return line
 
 
 # -- batched scenarios -------------------------------------------------------------------------------
@@ -932,6 +1213,124 @@ def run_adjoint(args, world: int, local: int) -> dict:
     return out
 
 
+def adjoint_fd_check(args, local: int) -> dict:
+    """The adjoint of the calibration problem at its benchmark size (250k cells, 32 knots, 200
+    gauges, checkpoints every 50 steps) over a shorter run (``--fd-steps``), against float64:
+
+    * directional derivatives along ``--fd-directions`` seeded random directions of (n, z, q)
+      by central differences of the float64 loss (the same discrete step in float64 on the GPU,
+      ``oracle/torch_step.py``, with the CUDA run's dt frozen), at two step sizes, the
+      direction counted as smooth where they agree to 1e-3;
+    * the CUDA gradient (derivatives cut below the film depth, 4 dry_tol) against those
+      differences of the exact loss: the cut surrogate's bias and the float32 error together;
+    * float64 autograd with the same cut against the same differences (the bias alone) and
+      against the CUDA gradient (the implementation's error alone).
+    Errors are relative to the summed size of the n, z and q terms of a direction.
+    """
+    import torch
+
+    from oracle.torch_step import TorchStep, hydrograph_value, misfit
+
+    device = f"cuda:{local}"
+    t_all = time.perf_counter()
+    sc, prob, n, z, q = _adjoint_problem(args.adjoint_cells, args.fd_steps, 32, 200, device)
+    true_dts, true_ts = prob.clock()
+    loss32 = prob.loss(n, z, q)
+    gn, gz, gq = prob.gradient()
+    dts, ts = prob.clock()
+    g = sc.geom
+    t64 = lambda a: torch.as_tensor(np.asarray(a, np.float64), device=device)  # noqa: E731
+    hg = sc.hydrographs[0]
+    cells = torch.as_tensor(np.asarray(hg.cells, np.int64), device=device)
+    hscale = t64((hg.shares() * (1.0 / np.asarray(g.area, np.float32)[hg.cells]).astype(np.float32)).astype(np.float64))
+    hydro = [(cells, hscale, t64(hg.knot_t), slice(0, hg.knot_q.size))]
+    gauges = torch.as_tensor(np.asarray(sc.meta["gauges"], np.int64), device=device)
+    exact = TorchStep(g, dry_tol=sc.dry_tol, device=device)
+    cut = TorchStep(g, dry_tol=sc.dry_tol, device=device, cut_depth=prob.cut_depth)
+    with torch.no_grad():  # the float64 model's own observations, with the "true" run's clock
+        dzL, dzR = exact.bed_steps(t64(z))
+        h, hu, hv = t64(sc.h0), t64(sc.hu0), t64(sc.hv0)
+        obs = []
+        for dt, t in zip(true_dts, true_ts, strict=True):
+            h, hu, hv = exact.step(h, hu, hv, t64(sc.meta["n_true"]), dzL, dzR, dt, cells,
+                                   hscale * hydrograph_value(t64(hg.knot_t), t64(q), t))
+            obs.append(h[gauges])
+        obs = torch.stack(obs)
+
+    def loss64(model, nn, zz, qq, grad=False):
+        return misfit(model, t64(sc.h0), t64(sc.hu0), t64(sc.hv0), nn, zz, qq, dts, ts, gauges, obs, hydro=hydro,
+                      checkpoint=grad)
+
+    n_t, z_t, q_t = (t64(v).requires_grad_(True) for v in (n, z, q))
+    loss_cut = loss64(cut, n_t, z_t, q_t, grad=True)
+    loss_cut.backward()
+    an, az, aq = (v.grad.cpu().numpy() for v in (n_t, z_t, q_t))
+    n0, z0, q0 = (np.asarray(v, np.float64) for v in (n, z, q))
+    rows = []
+    with torch.no_grad():
+        base = float(loss64(exact, t64(n0), t64(z0), t64(q0)))
+
+        def fd(dn, dz, dq, eps):
+            plus = float(loss64(exact, t64(n0 + eps * dn), t64(z0 + eps * dz), t64(q0 + eps * dq)))
+            minus = float(loss64(exact, t64(n0 - eps * dn), t64(z0 - eps * dz), t64(q0 - eps * dq)))
+            return (plus - minus) / (2.0 * eps)
+
+        for k in range(args.fd_directions):
+            rng = np.random.default_rng(500 + k)
+            dn = rng.standard_normal(n0.size) * 0.005
+            dz = rng.standard_normal(z0.size) * 0.01
+            dq = rng.standard_normal(q0.size) * 2.0
+            d1, d2 = fd(dn, dz, dq, 1e-5), fd(dn, dz, dq, 2e-6)
+            cuda = (float(np.dot(gn, dn)), float(np.dot(gz, dz)), float(np.dot(gq, dq)))
+            ref = (float(np.dot(an, dn)), float(np.dot(az, dz)), float(np.dot(aq, dq)))
+            scale = sum(abs(v) for v in cuda)
+            rows.append({
+                "direction": k,
+                "fd": d1,
+                "fd_fine": d2,
+                "smooth": abs(d1 - d2) <= 1e-3 * max(abs(d1), 1e-300),
+                "cuda_cut": sum(cuda),
+                "f64_cut": sum(ref),
+                "err_cuda_cut_vs_fd": abs(sum(cuda) - d1) / scale,
+                "err_f64_cut_vs_fd": abs(sum(ref) - d1) / scale,
+                "err_cuda_vs_f64_cut": abs(sum(cuda) - sum(ref)) / scale,
+            })
+    smooth = [r for r in rows if r["smooth"]]
+    rel = lambda a, b: float(np.linalg.norm(np.asarray(a, np.float64) - b) / np.linalg.norm(b))  # noqa: E731
+    med = lambda key, rs: float(np.median([r[key] for r in rs])) if rs else None  # noqa: E731
+    mx = lambda key, rs: float(np.max([r[key] for r in rs])) if rs else None  # noqa: E731
+    return {
+        "workload": f"calibration_{g.N // 1000}k_voronoi",
+        "cells": int(g.N),
+        "steps": int(prob.steps),
+        "checkpoint_every": int(prob.K),
+        "knots": int(prob.n_knots),
+        "gauges": int(prob.gauges.size),
+        "cut_depth_m": prob.cut_depth,
+        "loss_f32": loss32,
+        "loss_f64": base,
+        "grad_rel_vs_f64_cut_autograd": {"n": rel(gn, an), "z": rel(gz, az), "q": rel(gq, aq)},
+        "directions": len(rows),
+        "smooth_directions": len(smooth),
+        "smooth": {
+            "err_cuda_cut_vs_fd_median": med("err_cuda_cut_vs_fd", smooth),
+            "err_cuda_cut_vs_fd_max": mx("err_cuda_cut_vs_fd", smooth),
+            "err_f64_cut_vs_fd_median": med("err_f64_cut_vs_fd", smooth),
+            "err_f64_cut_vs_fd_max": mx("err_f64_cut_vs_fd", smooth),
+            "err_cuda_vs_f64_cut_max": mx("err_cuda_vs_f64_cut", smooth),
+        },
+        "all_directions": {
+            "err_cuda_cut_vs_fd_median": med("err_cuda_cut_vs_fd", rows),
+            "err_f64_cut_vs_fd_median": med("err_f64_cut_vs_fd", rows),
+            "err_cuda_vs_f64_cut_max": mx("err_cuda_vs_f64_cut", rows),
+        },
+        "rows": rows,
+        "wall_s": time.perf_counter() - t_all,
+        "reference": "float64 torch restatement of the same discrete step on the GPU (oracle/torch_step.py), dt "
+        "frozen at the CUDA run's values; central differences at eps 1e-5 and 2e-6 of the exact (uncut) loss",
+    }
+
+
 # -- reference arm ---------------------------------------------------------------------------------
 _WORKER: dict = {}
 
@@ -972,6 +1371,10 @@ def run_reference(args, world: int, rank: int) -> None:
     ctx = mp.get_context("spawn")
     with ctx.Pool(procs, initializer=_ref_worker_init,
                   initargs=(args.workload, cells, args.seed, args.spin_up)) as pool:
+        # the full workload's description, as the CUDA arm states it (built while the workers start)
+        full = build_scenario(args.workload, args.cells, args.seed)
+        config = workload_config(full, args, float(full.meta.get("cfl", 0.8)))
+        del full
         for _ in range(args.warmup):
             pool.map(_ref_worker_step, range(procs), chunksize=1)
         t0 = time.perf_counter()
@@ -980,13 +1383,6 @@ def run_reference(args, world: int, rank: int) -> None:
             total += sum(pool.map(_ref_worker_step, range(procs), chunksize=1))
         wall = time.perf_counter() - t0
     value = total / wall
-    sc_cfg = {
-        "workload": f"{args.workload}_{args.cells // 1000}k_voronoi",
-        "cells": args.cells,
-        "sample_cells_per_process": cells,
-        "parallelism": f"{procs} processes",
-        "seed": args.seed,
-    }
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -1001,12 +1397,17 @@ def run_reference(args, world: int, rank: int) -> None:
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic: seeded Voronoi mesh, fractal DEM",
-        "config": sc_cfg,
+        "config": config,
         "cpu_baseline": {
             "value": value,
             "unit": UNIT,
             "cores": procs,
             "kind": "port",
+            "source": "oracle/fp64_step.py: the reference's float64 CPU step tests/unit/_cpu_step.py restated, "
+            "pinned to that file's outputs to 1e-12 by tests/golden/cpu_step.npz (the reference keeps the step in "
+            "its test tree, which a package install does not carry, so the restatement runs)",
+            "sample_cells_per_process": cells,
+            "processes": procs,
             "sample": f"each step: one float64 Heun step of a {cells}-cell sample of the workload (same cell "
             f"size, terrain and water) in each of {procs} processes"
             + (f"; rain_inflow: a {1000 * 0.05 / 3600 * args.spin_up:.2f} mm film for the state the rain leaves "
@@ -1026,6 +1427,13 @@ def main() -> None:
         run_reference(args, world, rank)
         return
     world, rank, local = dist_setup()
+    if args.adjoint_fd:
+        import torch
+
+        torch.cuda.set_device(local)
+        if rank == 0:
+            print(json.dumps(adjoint_fd_check(args, local)), flush=True)
+        return
     try:
         run_b200(args, world, rank, local)
     finally:

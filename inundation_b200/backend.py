@@ -35,7 +35,7 @@ import numpy as np
 import torch
 from numpy.typing import NDArray
 
-from .engine import RESIDENT_CTRL_DTYPE, ResidentEngine
+from .engine import KERNELS, RESIDENT_CTRL_DTYPE, ResidentEngine
 from .layout import build_tile_layout
 from .mesh.geometry import MeshGeometry
 from .tuning import (
@@ -50,6 +50,20 @@ from .tuning import (
 )
 
 STEPS_PER_GRAPH_DEFAULT = 200
+KERNEL_NAMES = {v: k for k, v in KERNELS.items()}
+
+
+@dataclasses.dataclass(frozen=True)
+class SubmitRecord:
+    """One submit of a run: the clock after it, the steps it ran, the kernel that ran them and the
+    active blocks the dilation left for the next submit (what ``stage_kernel = "auto"`` reads)."""
+
+    now_ticks: int
+    steps: int
+    kernel: str
+    active_blocks: int
+    computed_cells: int  # cells of computed tiles over the run so far
+    wall_s: float  # host monotonic clock when the submit's control block was read
 
 
 class SWESolverB200Resident(ResidentEngine):
@@ -59,6 +73,8 @@ class SWESolverB200Resident(ResidentEngine):
     steps_per_graph: int = STEPS_PER_GRAPH_DEFAULT
     # Fixed-order gathers are the only accumulation: repeat runs are bit-identical.
     deterministic: bool = True
+    # A list to have run() append one SubmitRecord per submit (None: no record is kept).
+    submit_log: list[SubmitRecord] | None = None
 
     def __init__(
         self,
@@ -287,11 +303,17 @@ class SWESolverB200Resident(ResidentEngine):
             self._read_ctrl()
             while int(ctrl["now_ticks"][0]) < stop:
                 before = int(ctrl["now_ticks"][0])
-                graph = self._graph()  # per submit: "auto" may change kernel with the active fraction
+                steps_before = int(ctrl["steps"][0])
+                kernel = self._kernel  # per submit: "auto" may change kernel with the active fraction
+                graph = self._graph()
                 with torch.cuda.stream(self._stream):
                     graph.replay()
                 self._read_ctrl()
                 now_ticks = int(ctrl["now_ticks"][0])
+                if self.submit_log is not None:
+                    self.submit_log.append(SubmitRecord(now_ticks, int(ctrl["steps"][0]) - steps_before,
+                                                        KERNEL_NAMES[kernel], self._active_blocks,
+                                                        self._computed_cells_read(), _time.monotonic()))
                 if now_ticks == before:
                     raise RuntimeError(
                         f"GPU-resident run made no time progress at t={ticks_to_seconds(now_ticks):.6f}s "
@@ -343,4 +365,4 @@ class SWESolverB200Resident(ResidentEngine):
         sys.stdout.flush()
 
 
-__all__ = ["RESIDENT_CTRL_DTYPE", "STEPS_PER_GRAPH_DEFAULT", "SWESolverB200Resident"]
+__all__ = ["RESIDENT_CTRL_DTYPE", "STEPS_PER_GRAPH_DEFAULT", "SWESolverB200Resident", "SubmitRecord"]

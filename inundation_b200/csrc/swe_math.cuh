@@ -122,26 +122,24 @@ __device__ __forceinline__ void hllc(const Phys &p, float hL, float hqnL, float 
     const float num_sm = SL * hR * (unR - SR) - SR * hL * (unL - SL);
     const float den_sm = hR * (unR - SR) - hL * (unL - SL);
     const float SM = (fabsf(den_sm) > 1e-12f) ? num_sm / den_sm : 0.0f;
-    if (SL >= 0.0f) {
-        Fh = hL * unL;
-        Fhn = hL * unL * unL + 0.5f * p.g * hL * hL;
-        Fht = hL * unL * utL;
-    } else if (SM >= 0.0f) {
-        const float dSL = SL - SM;
-        const float kL = hL * (SL - unL) / ((fabsf(dSL) > 1e-14f) ? dSL : 1e-14f);
-        Fh = hL * unL + SL * (kL - hL);
-        Fhn = (hL * unL * unL + 0.5f * p.g * hL * hL) + SL * (kL * SM - hL * unL);
-        Fht = hL * unL * utL + SL * (kL * utL - hL * utL);
-    } else if (SR >= 0.0f) {
-        const float dSR = SR - SM;
-        const float kR = hR * (SR - unR) / ((fabsf(dSR) > 1e-14f) ? dSR : 1e-14f);
-        Fh = hR * unR + SR * (kR - hR);
-        Fhn = (hR * unR * unR + 0.5f * p.g * hR * hR) + SR * (kR * SM - hR * unR);
-        Fht = hR * unR * utR + SR * (kR * utR - hR * utR);
-    } else {
-        Fh = hR * unR;
-        Fhn = hR * unR * unR + 0.5f * p.g * hR * hR;
-        Fht = hR * unR * utR;
+    // The four regions (SL >= 0: left; SM >= 0: left star; SR >= 0: right star; else right)
+    // share one side's plain flux and, in the star regions, one correction: the side is
+    // selected first, so a warp whose edges fall in both star regions runs the star
+    // arithmetic once, with the same operations on the same values as per region.
+    const bool left = (SL >= 0.0f) || (SM >= 0.0f);
+    const bool star = !(SL >= 0.0f) && (left || SR >= 0.0f);
+    const float h = left ? hL : hR, un = left ? unL : unR, ut = left ? utL : utR;
+    const float q = h * un;
+    Fh = q;
+    Fhn = q * un + 0.5f * p.g * h * h;
+    Fht = q * ut;
+    if (star) {
+        const float S = left ? SL : SR;
+        const float dS = S - SM;
+        const float k = h * (S - un) / ((fabsf(dS) > 1e-14f) ? dS : 1e-14f);
+        Fh = q + S * (k - h);
+        Fhn = Fhn + S * (k * SM - q);
+        Fht = Fht + S * (k * ut - h * ut);
     }
 }
 

@@ -441,6 +441,10 @@ class ResidentEngine:
                                                    (4, "for a step's dt")) if err & bit)
             raise RuntimeError(f"{B200_BACKEND}: a bounded device wait {what} timed out (error {err})")
 
+    def _computed_cells_read(self) -> int:
+        """The computed-cells total as of the last control-block read (no device access)."""
+        return int(self._sched_pinned.numpy().view(np.uint64)[3])
+
     def _enqueue_prologue(self) -> None:
         p = self._params()
         with torch.cuda.stream(self._stream):

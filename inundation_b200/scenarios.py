@@ -94,7 +94,7 @@ def dam_break(n_cells: int = 1_000_000, seed: int = 2, side: float = 10_000.0) -
     h0 = np.where(r <= 0.05 * side, 4.0, 0.0).astype(np.float32)
     z = np.zeros(geom.N, np.float32)
     return Scenario("dam_break", geom, h0, z, z.copy(), np.full(geom.N, 0.035, np.float32), t_end=3600.0,
-                    meta={"radius_m": 0.05 * side, "depth_m": 4.0})
+                    meta={"radius_m": 0.05 * side, "depth_m": 4.0, "centre_m": (side / 2, side / 2)})
 
 
 def triangular_hydrograph(t: NDArray[np.float64] | float, peak: float, t_peak: float, t_end: float):

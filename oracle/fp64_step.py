@@ -198,3 +198,57 @@ def run_steps(geom, h, hu, hv, n, dt: float, steps: int, *, g: float, dry_tol: f
     for _ in range(steps):
         s = heun_step(geom, s, n64, dt, g=g, dry_tol=dry_tol)
     return s
+
+
+@dataclass(frozen=True)
+class Region:
+    """The cells ``cells`` of a mesh as a mesh of their own, for the step functions above.
+
+    Edges keep their order; an edge with one cell outside the region becomes a
+    wall of the inside cell (oriented outward from it). The steps above give
+    the same values on a region as on the whole mesh for as long as no water
+    reaches a cell with such an edge: every edge across the region's rim is
+    then dry on both sides, which the whole-mesh step skips as well.
+    """
+
+    N: int
+    edge_cellL: NDArray[np.int64]
+    edge_cellR: NDArray[np.int64]
+    edge_nx: NDArray[np.float32]
+    edge_ny: NDArray[np.float32]
+    edge_len: NDArray[np.float32]
+    zb: NDArray[np.float32]
+    area: NDArray[np.float32]
+    cells: NDArray[np.int64]  # region cell -> mesh cell
+    rim: NDArray[np.int64]  # region cells with an edge to a cell outside
+
+
+def restrict(geom, cells: NDArray[np.int64]) -> Region:
+    cells = np.unique(np.asarray(cells, np.int64))
+    inside = np.zeros(geom.N, bool)
+    inside[cells] = True
+    local = np.full(geom.N, -1, np.int64)
+    local[cells] = np.arange(cells.size)
+    cL = np.asarray(geom.edge_cellL, np.int64)
+    cR = np.asarray(geom.edge_cellR, np.int64)
+    in_l = inside[cL]
+    in_r = (cR >= 0) & inside[np.where(cR >= 0, cR, 0)]
+    keep = in_l | in_r
+    flip = keep & ~in_l  # the right cell is the inside one: it becomes the left cell of a wall
+    cut = keep & in_l & (cR >= 0) & ~in_r
+    new_l = np.where(flip, local[np.where(cR >= 0, cR, 0)], local[cL])[keep]
+    new_r = np.where(flip | cut, -1, np.where(cR >= 0, local[np.where(cR >= 0, cR, 0)], -1))[keep]
+    sign = np.where(flip, -1.0, 1.0)[keep].astype(np.float32)
+    rim = np.unique(np.concatenate([local[cL[cut]], local[cR[flip]]]))
+    return Region(
+        N=int(cells.size),
+        edge_cellL=new_l,
+        edge_cellR=new_r,
+        edge_nx=np.asarray(geom.edge_nx)[keep] * sign,
+        edge_ny=np.asarray(geom.edge_ny)[keep] * sign,
+        edge_len=np.asarray(geom.edge_len)[keep],
+        zb=np.asarray(geom.zb)[cells],
+        area=np.asarray(geom.area)[cells],
+        cells=cells,
+        rim=rim,
+    )

@@ -57,3 +57,16 @@ def test_small_workloads_and_their_config(workload: str) -> None:
     else:
         assert wet.any()
 
+
+
+def test_reference_arm_states_the_cuda_arms_config(capsys: pytest.CaptureFixture[str]) -> None:
+    """Both arms print the same ``config`` for the same workload, so their lines compare directly."""
+    import json
+
+    args = args_for("dam_break", "--impl", "reference", "--cells", "3000", "--steps", "1", "--warmup", "1")
+    bench.run_reference(args, world=1, rank=0)
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    sc = bench.build_scenario("dam_break", args.cells, args.seed)
+    assert line["config"] == json.loads(json.dumps(bench.workload_config(sc, args, 0.8)))
+    assert line["impl"] == "reference" and line["cpu_baseline"]["kind"] == "port"
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["value"] > 0

@@ -227,3 +227,23 @@ def test_closed_basin_conserves_volume_with_compensation() -> None:
     o.run(t_end=20.0, output_interval_s=10.0, dt_max=1.0, dt_init=0.01)
     assert o.steps_total > 50
     assert float((o.download_h_precise() * g.area).sum()) == pytest.approx(v0, rel=1e-6)
+
+
+def test_a_region_steps_like_the_whole_mesh_while_its_rim_stays_dry() -> None:
+    """``fp64_step.restrict``: the float64 step over a region equals the whole mesh's there, bit for bit."""
+    from tests._valley import dam, valley_grid
+
+    g = valley_grid(nx=64, ny=32)
+    h0 = dam(g, 64, 32).astype(np.float64)
+    cells = np.flatnonzero(g.centroid[:, 0] < 64 * 2.0 * 0.6)
+    region = fp64_step.restrict(g, cells)
+    assert region.N == cells.size and region.rim.size > 0
+    n = np.full(g.N, 0.03)
+    whole = fp64_step.State(h0, 0 * h0, 0 * h0)
+    part = fp64_step.State(h0[cells], 0 * h0[cells], 0 * h0[cells])
+    for _ in range(40):
+        whole = fp64_step.heun_step(g, whole, n, 2.0**-6, g=9.81, dry_tol=1e-3)
+        part = fp64_step.heun_step(region, part, n[cells], 2.0**-6, g=9.81, dry_tol=1e-3)
+    assert part.h[region.rim].max() == 0.0 and whole.h[np.setdiff1d(np.arange(g.N), cells)].max() == 0.0
+    for a, b in ((whole.h, part.h), (whole.hu, part.hu), (whole.hv, part.hv)):
+        np.testing.assert_array_equal(a[cells], b)
