@@ -351,8 +351,10 @@ int swe_open_ghost_probe(const float *cases, const uint32_t *cond, float *result
    control block. For tests of the limit: no counterpart in the reference. */
 int swe_dt_wait_probe(const swe_state_t *state, uint32_t epoch, uint32_t *out, swe_stream_t stream);
 
-/* (x^(4/3)) of n values on the device, the Manning depth power the update uses. */
-int swe_pow43(const float *x, float *out, uint32_t n, swe_stream_t stream);
+/* x^(-4/3) of n values on the device, the depth power of the Manning friction slope
+   (Sf = g n^2 |u| h^(-4/3)) as the update evaluates it. Replaces the pow(h, 4/3) of
+   update_resident_gather (resident.py:489-495), for tests of its accuracy. */
+int swe_inv_pow43(const float *x, float *out, uint32_t n, swe_stream_t stream);
 
 const char *swe_status_string(int status);
 

@@ -52,7 +52,7 @@ struct CellFwd {
     float h_new, lo_new, hu_new, hv_new;  // outputs
     float hu_a, hv_a;                     // momenta before drag and friction
     float drag, hu_b, hv_b;               // after drag
-    float spd, P, Sf, den, u, v;          // friction
+    float spd, Q, Sf, den, u, v;          // friction (Q = h^(-4/3))
     bool clamped, wet;
 };
 
@@ -61,13 +61,13 @@ __device__ __forceinline__ CellFwd cell_forward(const Phys &p, float dt, float A
     CellFwd c;
     const float dti = dt / A;
     c.clamped = add_compensated_clamped(hi, loi, -dti * sdh, c.h_new, c.lo_new);
-    c.hu_a = hui - dti * sdhu;
-    c.hv_a = hvi - dti * sdhv;
+    c.hu_a = fmaf_rn(-dti, sdhu, hui);
+    c.hv_a = fmaf_rn(-dti, sdhv, hvi);
     c.wet = !(c.h_new < p.dry_tol);
     c.drag = 1.0f;
     c.hu_b = c.hu_a;
     c.hv_b = c.hv_a;
-    c.spd = c.P = c.Sf = c.u = c.v = 0.0f;
+    c.spd = c.Q = c.Sf = c.u = c.v = 0.0f;
     c.den = 1.0f;
     if (!c.wet) {
         c.hu_new = 0.0f;
@@ -80,10 +80,10 @@ __device__ __forceinline__ CellFwd cell_forward(const Phys &p, float dt, float A
     const float inv_h = 1.0f / c.h_new;
     c.u = c.hu_b * inv_h;
     c.v = c.hv_b * inv_h;
-    c.spd = sqrtf(c.u * c.u + c.v * c.v);
-    c.P = pow43(c.h_new);
-    c.Sf = p.g * n * n * c.spd / c.P;
-    c.den = 1.0f + dt * c.Sf;
+    c.spd = sqrtf(fmaf_rn(c.u, c.u, c.v * c.v));
+    c.Q = inv_pow43(c.h_new);
+    c.Sf = p.g * n * n * c.spd * c.Q;
+    c.den = fmaf_rn(dt, c.Sf, 1.0f);
     const float inv_den = 1.0f / c.den;
     c.hu_new = c.hu_b * inv_den;
     c.hv_new = c.hv_b * inv_den;
@@ -103,10 +103,10 @@ __device__ __forceinline__ void cell_reverse(const Phys &p, float dt, float A, f
         float g_hub = gHU / c.den, g_hvb = gHV / c.den;
         const float g_den = -(gHU * c.hu_new + gHV * c.hv_new) / c.den;
         const float g_Sf = g_den * dt;
-        g_n += g_Sf * 2.0f * p.g * n * c.spd / c.P;
-        const float g_spd = g_Sf * p.g * n * n / c.P;
-        const float g_P = -g_Sf * c.Sf / c.P;
-        if (!thin) gH += g_P * (4.0f / 3.0f) * c.P / h;
+        g_n += g_Sf * 2.0f * p.g * n * c.spd * c.Q;
+        const float g_spd = g_Sf * p.g * n * n * c.Q;
+        // Sf is proportional to h^(-4/3): d Sf / dh = -(4/3) Sf / h
+        if (!thin) gH -= g_Sf * c.Sf * (4.0f / 3.0f) / h;
         if (c.spd > 0.0f) {
             const float g_u = g_spd * c.u / c.spd, g_v = g_spd * c.v / c.spd;
             g_hub += g_u / h;
@@ -169,20 +169,21 @@ __device__ EdgeGrad edge_words_rev(const Phys &p, bool wall, float nx, float ny,
     safe_vel2(p, hL, huL, hvL, uL, vL);
     safe_vel2(p, hR, huR, hvR, uR, vR);
     const float huLs = hLs * uL, hvLs = hLs * vL, huRs = hRs * uR, hvRs = hRs * vR;
-    const float hqnL = huLs * nx + hvLs * ny;
-    const float hqtL = -huLs * ny + hvLs * nx;
-    const float hqnR = huRs * nx + hvRs * ny;
-    const float hqtR = -huRs * ny + hvRs * nx;
+    const float hqnL = fmaf_rn(huLs, nx, hvLs * ny);
+    const float hqtL = fmaf_rn(hvLs, nx, -(huLs * ny));
+    const float hqnR = fmaf_rn(huRs, nx, hvRs * ny);
+    const float hqtR = fmaf_rn(hvRs, nx, -(huRs * ny));
     float unL, utL, unR, utR;
     safe_vel2(p, hLs, hqnL, hqtL, unL, utL);
     safe_vel2(p, hRs, hqnR, hqtR, unR, utR);
-    const float cL = sqrtf(p.g * gmax(hLs, 0.0f));
-    const float cR = sqrtf(p.g * gmax(hRs, 0.0f));
     const float sqL = sqrtf(gmax(hLs, 0.0f));
     const float sqR = sqrtf(gmax(hRs, 0.0f));
+    const float root_g = sqrtf(p.g);
+    const float cL = root_g * sqL;
+    const float cR = root_g * sqR;
     const float den = sqL + sqR;
     const bool roe_ok = den > 1e-12f;
-    const float u_roe = roe_ok ? (sqL * unL + sqR * unR) / den : 0.0f;
+    const float u_roe = roe_ok ? fmaf_rn(sqL, unL, sqR * unR) / den : 0.0f;
     const float c_roe = sqrtf(p.g * 0.5f * (hLs + hRs));
     const float aL = unL - cL, bL = u_roe - c_roe;
     const bool selL = bL < aL;
@@ -195,10 +196,11 @@ __device__ EdgeGrad edge_words_rev(const Phys &p, bool wall, float nx, float ny,
     const float dryLeft = (1.0f - wetL) * wetR;
     const float dryRight = (1.0f - wetR) * wetL;
     const float roe = 1.0f - dryLeft - dryRight;
-    const float SL = roe * SL0 + dryLeft * (unR - 2.0f * cR) + dryRight * (unL - cL);
-    const float SR = roe * SR0 + dryLeft * (unR + cR) + dryRight * (unL + 2.0f * cL);
-    const float num_sm = SL * hRs * (unR - SR) - SR * hLs * (unL - SL);
-    const float den_sm = hRs * (unR - SR) - hLs * (unL - SL);
+    const float SL = fmaf_rn(roe, SL0, fmaf_rn(dryLeft, fmaf_rn(-2.0f, cR, unR), dryRight * (unL - cL)));
+    const float SR = fmaf_rn(roe, SR0, fmaf_rn(dryLeft, unR + cR, dryRight * fmaf_rn(2.0f, cL, unL)));
+    const float aRs = hRs * (unR - SR), aLs = hLs * (unL - SL);
+    const float num_sm = fmaf_rn(SL, aRs, -(SR * aLs));
+    const float den_sm = aRs - aLs;
     const bool sm_ok = fabsf(den_sm) > 1e-12f;
     const float SM = sm_ok ? num_sm / den_sm : 0.0f;
     const int branch = (SL >= 0.0f) ? 0 : (SM >= 0.0f) ? 1 : (SR >= 0.0f) ? 2 : 3;

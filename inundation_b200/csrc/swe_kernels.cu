@@ -54,8 +54,8 @@ __global__ void eft_probe_kernel(float *v) {
     v[2] = ee;
 }
 
-__global__ void pow43_kernel(const float *x, float *out, uint32_t n) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = pow43(x[i]);
+__global__ void inv_pow43_kernel(const float *x, float *out, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = inv_pow43(x[i]);
 }
 
 // The ghost state and mass flux of open edges from given cells: the device
@@ -118,9 +118,9 @@ int swe_eft_probe(float *v, swe_stream_t stream) {
     return check_launch();
 }
 
-int swe_pow43(const float *x, float *out, uint32_t n, swe_stream_t stream) {
+int swe_inv_pow43(const float *x, float *out, uint32_t n, swe_stream_t stream) {
     if (!x || !out || n == 0u) return SWE_ERR_ARGUMENT;
-    pow43_kernel<<<min((n + 255u) / 256u, 4096u), 256, 0, stream>>>(x, out, n);
+    inv_pow43_kernel<<<min((n + 255u) / 256u, 4096u), 256, 0, stream>>>(x, out, n);
     return check_launch();
 }
 

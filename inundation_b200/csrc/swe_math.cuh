@@ -1,10 +1,14 @@
 // Device arithmetic of the shallow-water step, in float32.
 //
-// Each function evaluates the same expression, in the same order, as the
-// reference's GLSL (inundation/vulkan/shaders/flux.py:43-182 and 301-319), so
-// that with contraction off (--fmad=false) and IEEE division and square root
-// every result is reproducible bit for bit. GLSL min/max/clamp are written
-// with their specified comparisons: min(x,y) = y<x ? y : x, max(x,y) = x<y ? y : x.
+// Each function evaluates the reference's GLSL expression
+// (inundation/vulkan/shaders/flux.py:43-182 and 301-319) in a stated order:
+// contraction is off (--fmad=false), so the only fused multiply-adds are the
+// explicit fmaf_rn() calls, and division and square root are IEEE. The FP32
+// oracle (oracle/fp32_resident.c) evaluates the same expressions with C's
+// fmaf, sqrtf and division, so every result is reproducible bit for bit.
+// GLSL contracts a*b+c freely outside `precise` blocks, so a fused site is a
+// value the reference admits. GLSL min/max/clamp are written with their
+// specified comparisons: min(x,y) = y<x ? y : x, max(x,y) = x<y ? y : x.
 #pragma once
 #include <cstdint>
 
@@ -19,6 +23,7 @@ struct Phys {
     float dry_tol;
 };
 
+__device__ __forceinline__ float fmaf_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ float gmin(float x, float y) { return (y < x) ? y : x; }
 __device__ __forceinline__ float gmax(float x, float y) { return (x < y) ? y : x; }
 __device__ __forceinline__ float gclamp(float x, float lo, float hi) { return gmin(gmax(x, lo), hi); }
@@ -29,14 +34,21 @@ __device__ __forceinline__ float gclamp(float x, float lo, float hi) { return gm
 // evaluate the same expressions.
 constexpr float kOneThird = 1.0f / 3.0f;
 
-// x^(4/3) for x > 0: cube root by Newton's iteration r <- (2r + x/r^2) * (1/3)
-// from the exponent-thirds estimate bits(x)/3 + (2/3)*127*2^23, then x*r.
-// Basic IEEE operations only, so host and device agree exactly.
-__device__ __forceinline__ float pow43(float x) {
-    float r = __uint_as_float(__float_as_uint(x) / 3u + 0x2A555555u);
+// x^(-4/3) for x > 0, the depth power of Manning's friction slope (Sf = g n^2 |u| / h^(4/3)),
+// without a division: y = x^(-1/3) by Newton's iteration for 1/y^3 = x,
+//   y <- y + (y/3)(1 - x y^3),
+// from the exponent-thirds estimate bits(y) = (4/3)*127*2^23 - bits(x)/3; four steps
+// converge from that estimate's error, then x^(-4/3) = (y^2)^2. Within 6 ulp of the exact
+// power over [1e-12, 1e6]. Multiplies and fused multiply-adds only, so host and device agree.
+__device__ __forceinline__ float inv_pow43(float x) {
+    float y = __uint_as_float(0x54AAAAAAu - __float_as_uint(x) / 3u);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) r = (2.0f * r + x / (r * r)) * kOneThird;
-    return x * r;
+    for (int k = 0; k < 4; ++k) {
+        const float t = x * (y * y);
+        y = fmaf_rn(y * kOneThird, fmaf_rn(-t, y, 1.0f), y);
+    }
+    const float y2 = y * y;
+    return y2 * y2;
 }
 
 // Desingularised velocity (Kurganov & Petrova 2007): hq/h above the film depth.
@@ -62,12 +74,13 @@ __device__ __forceinline__ void safe_vel2(const Phys &p, float h, float hq1, flo
 // dry-bed speeds u -+ 2c as a side goes from one to two dry_tol deep.
 __device__ __forceinline__ void hllc_speeds(const Phys &p, float hL, float unL, float hR, float unR, float &SLo,
                                             float &SRo) {
-    const float cL = sqrtf(p.g * gmax(hL, 0.0f));
-    const float cR = sqrtf(p.g * gmax(hR, 0.0f));
     const float sqL = sqrtf(gmax(hL, 0.0f));
     const float sqR = sqrtf(gmax(hR, 0.0f));
+    const float root_g = sqrtf(p.g);  // loop-invariant: hoisted out of the callers' edge loops
+    const float cL = root_g * sqL;
+    const float cR = root_g * sqR;
     const float den = sqL + sqR;
-    const float u_roe = (den > 1e-12f) ? (sqL * unL + sqR * unR) / den : 0.0f;
+    const float u_roe = (den > 1e-12f) ? fmaf_rn(sqL, unL, sqR * unR) / den : 0.0f;
     const float c_roe = sqrtf(p.g * 0.5f * (hL + hR));
     const float SL = gmin(unL - cL, u_roe - c_roe);
     const float SR = gmax(unR + cR, u_roe + c_roe);
@@ -76,8 +89,8 @@ __device__ __forceinline__ void hllc_speeds(const Phys &p, float hL, float unL, 
     const float dryLeft = (1.0f - wetL) * wetR;
     const float dryRight = (1.0f - wetR) * wetL;
     const float roe = 1.0f - dryLeft - dryRight;
-    SLo = roe * SL + dryLeft * (unR - 2.0f * cR) + dryRight * (unL - cL);
-    SRo = roe * SR + dryLeft * (unR + cR) + dryRight * (unL + 2.0f * cL);
+    SLo = fmaf_rn(roe, SL, fmaf_rn(dryLeft, fmaf_rn(-2.0f, cR, unR), dryRight * (unL - cL)));
+    SRo = fmaf_rn(roe, SR, fmaf_rn(dryLeft, unR + cR, dryRight * fmaf_rn(2.0f, cL, unL)));
 }
 
 // clamp(h / dry_tol - 1, 0, 1) without the division where its value is known:
@@ -92,12 +105,13 @@ __device__ __forceinline__ float wet_blend(const Phys &p, float h) {
 // hllc_speeds with wet_blend for the two blend weights: the same values, bit for bit.
 __device__ __forceinline__ void hllc_speeds_fast(const Phys &p, float hL, float unL, float hR, float unR, float &SLo,
                                                  float &SRo) {
-    const float cL = sqrtf(p.g * gmax(hL, 0.0f));
-    const float cR = sqrtf(p.g * gmax(hR, 0.0f));
     const float sqL = sqrtf(gmax(hL, 0.0f));
     const float sqR = sqrtf(gmax(hR, 0.0f));
+    const float root_g = sqrtf(p.g);  // loop-invariant: hoisted out of the callers' edge loops
+    const float cL = root_g * sqL;
+    const float cR = root_g * sqR;
     const float den = sqL + sqR;
-    const float u_roe = (den > 1e-12f) ? (sqL * unL + sqR * unR) / den : 0.0f;
+    const float u_roe = (den > 1e-12f) ? fmaf_rn(sqL, unL, sqR * unR) / den : 0.0f;
     const float c_roe = sqrtf(p.g * 0.5f * (hL + hR));
     const float SL = gmin(unL - cL, u_roe - c_roe);
     const float SR = gmax(unR + cR, u_roe + c_roe);
@@ -106,8 +120,8 @@ __device__ __forceinline__ void hllc_speeds_fast(const Phys &p, float hL, float 
     const float dryLeft = (1.0f - wetL) * wetR;
     const float dryRight = (1.0f - wetR) * wetL;
     const float roe = 1.0f - dryLeft - dryRight;
-    SLo = roe * SL + dryLeft * (unR - 2.0f * cR) + dryRight * (unL - cL);
-    SRo = roe * SR + dryLeft * (unR + cR) + dryRight * (unL + 2.0f * cL);
+    SLo = fmaf_rn(roe, SL, fmaf_rn(dryLeft, fmaf_rn(-2.0f, cR, unR), dryRight * (unL - cL)));
+    SRo = fmaf_rn(roe, SR, fmaf_rn(dryLeft, unR + cR, dryRight * fmaf_rn(2.0f, cL, unL)));
 }
 
 // HLLC flux in the face frame (Toro 2001); smax is the largest speed assumed.
@@ -119,8 +133,9 @@ __device__ __forceinline__ void hllc(const Phys &p, float hL, float hqnL, float 
     float SL, SR;
     hllc_speeds_fast(p, hL, unL, hR, unR, SL, SR);
     smax = gmax(fabsf(SL), fabsf(SR));
-    const float num_sm = SL * hR * (unR - SR) - SR * hL * (unL - SL);
-    const float den_sm = hR * (unR - SR) - hL * (unL - SL);
+    const float aR = hR * (unR - SR), aL = hL * (unL - SL);
+    const float num_sm = fmaf_rn(SL, aR, -(SR * aL));
+    const float den_sm = aR - aL;
     const float SM = (fabsf(den_sm) > 1e-12f) ? num_sm / den_sm : 0.0f;
     // The four regions (SL >= 0: left; SM >= 0: left star; SR >= 0: right star; else right)
     // share one side's plain flux and, in the star regions, one correction: the side is
@@ -131,15 +146,15 @@ __device__ __forceinline__ void hllc(const Phys &p, float hL, float hqnL, float 
     const float h = left ? hL : hR, un = left ? unL : unR, ut = left ? utL : utR;
     const float q = h * un;
     Fh = q;
-    Fhn = q * un + 0.5f * p.g * h * h;
+    Fhn = fmaf_rn(q, un, 0.5f * p.g * h * h);
     Fht = q * ut;
     if (star) {
         const float S = left ? SL : SR;
         const float dS = S - SM;
         const float k = h * (S - un) / ((fabsf(dS) > 1e-14f) ? dS : 1e-14f);
-        Fh = q + S * (k - h);
-        Fhn = Fhn + S * (k * SM - q);
-        Fht = Fht + S * (k * ut - h * ut);
+        Fh = fmaf_rn(S, k - h, q);
+        Fhn = fmaf_rn(S, fmaf_rn(k, SM, -q), Fhn);
+        Fht = fmaf_rn(S, (k - h) * ut, Fht);
     }
 }
 
@@ -154,10 +169,10 @@ __device__ __forceinline__ void face_states(const Phys &p, float hL, float huL, 
     safe_vel2(p, hL, huL, hvL, uL, vL);
     safe_vel2(p, hR, huR, hvR, uR, vR);
     const float huLs = hLs * uL, hvLs = hLs * vL, huRs = hRs * uR, hvRs = hRs * vR;
-    hqnL = huLs * nx + hvLs * ny;
-    hqtL = -huLs * ny + hvLs * nx;
-    hqnR = huRs * nx + hvRs * ny;
-    hqtR = -huRs * ny + hvRs * nx;
+    hqnL = fmaf_rn(huLs, nx, hvLs * ny);
+    hqtL = fmaf_rn(hvLs, nx, -(huLs * ny));
+    hqnR = fmaf_rn(huRs, nx, hvRs * ny);
+    hqtR = fmaf_rn(hvRs, nx, -(huRs * ny));
 }
 
 // The CFL wave speed the flux would assume on an edge.
@@ -171,8 +186,9 @@ __device__ __forceinline__ float wave_bound(const Phys &p, float hL, float huL, 
 
 // Wall ghost: the left state mirrored in the normal direction.
 __device__ __forceinline__ void wall_mirror(float huL, float hvL, float nx, float ny, float &huR, float &hvR) {
-    huR = huL - 2.0f * (huL * nx + hvL * ny) * nx;
-    hvR = hvL - 2.0f * (huL * nx + hvL * ny) * ny;
+    const float twice = -2.0f * fmaf_rn(huL, nx, hvL * ny);
+    huR = fmaf_rn(twice, nx, huL);
+    hvR = fmaf_rn(twice, ny, hvL);
 }
 
 // -- open boundaries (flux.py:187-294) ----------------------------------------------------------

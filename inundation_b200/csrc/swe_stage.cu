@@ -50,8 +50,13 @@ inline size_t block_smem_bytes(uint32_t max_tile_edges) {
 // sdhv at sums[i], sums[n + i], sums[2n + i], n = padded cells), the record
 // the adjoint reverses. OPEN: the mesh has open edges.
 // ---------------------------------------------------------------------------
+// CTAs of the block kernel that must fit on one SM (registers per thread follow from it).
+#ifndef SWE_BLOCK_MIN_CTAS
+#define SWE_BLOCK_MIN_CTAS 1
+#endif
+
 template <int STAGE, bool COMP, bool CLAMP, bool OPEN>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, SWE_BLOCK_MIN_CTAS)
     stage_block_kernel(swe_mesh_t m, swe_state_t s, Phys p, float cfl, float *sums) {
     const uint32_t cap = (m.max_tile_edges + 3u) & ~3u;
     const TileSmem t = tile_smem(cap);

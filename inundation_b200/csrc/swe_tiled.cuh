@@ -32,8 +32,8 @@ __device__ __forceinline__ void update_cell(const swe_state_t &s, const Phys &p,
         h_new = gmax(h_raw, 0.0f);
         lo_new = 0.0f;
     }
-    float hu_new = hui - dti * sdhu;
-    float hv_new = hvi - dti * sdhv;
+    float hu_new = fmaf_rn(-dti, sdhu, hui);
+    float hv_new = fmaf_rn(-dti, sdhv, hvi);
     if (CLAMP) s.clamp_mass[i] += 0.5f * A * (h_new - h_raw);
     if (h_new < p.dry_tol) {
         hu_new = 0.0f;
@@ -45,9 +45,9 @@ __device__ __forceinline__ void update_cell(const swe_state_t &s, const Phys &p,
         hv_new *= drag;
         const float inv_h = 1.0f / h_new;
         const float u_ = hu_new * inv_h, v_ = hv_new * inv_h;
-        const float spd = sqrtf(u_ * u_ + v_ * v_);
-        const float Sf = p.g * n * n * spd / pow43(h_new);
-        const float inv_den = 1.0f / (1.0f + dt * Sf);
+        const float spd = sqrtf(fmaf_rn(u_, u_, v_ * v_));
+        const float Sf = p.g * n * n * spd * inv_pow43(h_new);
+        const float inv_den = 1.0f / fmaf_rn(dt, Sf, 1.0f);
         hu_new = hu_new * inv_den;
         hv_new = hv_new * inv_den;
     }
@@ -118,15 +118,15 @@ __device__ __forceinline__ void edge_words(const Phys &p, int cR, float nx, floa
     } else if (cR < 0) {
         Fh = 0.0f;  // a wall passes no mass
     }
-    const float Fhu = Fhn * nx - Fht * ny;
-    const float Fhv = Fhn * ny + Fht * nx;
-    const float SL_g = 0.5f * p.g * (hL * hL - hLs * hLs);
-    const float SR_g = 0.5f * p.g * (hR * hR - hRs * hRs);
+    const float Fhu = fmaf_rn(Fhn, nx, -(Fht * ny));
+    const float Fhv = fmaf_rn(Fhn, ny, Fht * nx);
+    const float SL_g = 0.5f * p.g * fmaf_rn(hL, hL, -(hLs * hLs));
+    const float SR_g = 0.5f * p.g * fmaf_rn(hR, hR, -(hRs * hRs));
     w0 = Fh * len;
-    w1 = Fhu * len + SL_g * nx * len;
-    w2 = Fhv * len + SL_g * ny * len;
-    w3 = Fhu * len + SR_g * nx * len;
-    w4 = Fhv * len + SR_g * ny * len;
+    w1 = fmaf_rn(SL_g, nx, Fhu) * len;
+    w2 = fmaf_rn(SL_g, ny, Fhv) * len;
+    w3 = fmaf_rn(SR_g, nx, Fhu) * len;
+    w4 = fmaf_rn(SR_g, ny, Fhv) * len;
     w5 = smax * len;
 }
 // ---------------------------------------------------------------------------

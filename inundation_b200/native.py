@@ -40,7 +40,7 @@ _SIGNATURES: dict[str, tuple[list, object]] = {
     "swe_volume_fp64_noalloc": ([_P, _P, _P, _U32, _P, _P], ctypes.c_int),
     "swe_eft_probe": ([_P, _P], ctypes.c_int),
     "swe_dt_wait_probe": ([_P, _U32, _P, _P], ctypes.c_int),
-    "swe_pow43": ([_P, _P, _U32, _P], ctypes.c_int),
+    "swe_inv_pow43": ([_P, _P, _U32, _P], ctypes.c_int),
     "swe_open_ghost_probe": ([_P, _P, _P, _U32, ctypes.c_float, ctypes.c_float, _P], ctypes.c_int),
     "swe_status_string": ([ctypes.c_int], ctypes.c_char_p),
     "swe_bed_steps": ([_P, _P, _P, _P, _U32, _P, _P, _U32, _P], ctypes.c_int),

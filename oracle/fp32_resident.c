@@ -24,12 +24,16 @@
  *                                  edge as the reference's base solver keeps
  *                                  them (inundation/vulkan/solver.py:432-440)
  *
- * Every expression keeps the GLSL evaluation order; it is compiled with
- * -ffp-contract=off so no multiply-add is fused. GLSL min/max/clamp are
- * spelled out with their specified comparisons (min(x,y) = y<x ? y : x,
- * max(x,y) = x<y ? y : x). GLSL's pow has no fixed rounding, so
- * pow(h, 4/3) is evaluated by the same cube-root Newton sequence as the CUDA
- * kernels (pow43 below): a value the reference admits, bit-identical to the
+ * Every expression is evaluated in a stated order, the same as the CUDA
+ * kernels': it is compiled with -ffp-contract=off, so the only fused
+ * multiply-adds are the explicit fmaf() calls, at the kernels' sites (GLSL
+ * contracts a*b+c freely outside `precise` blocks, so a fused site is a value
+ * the reference admits; C's fmaf and CUDA's __fmaf_rn both round once).
+ * GLSL min/max/clamp are spelled out with their specified comparisons
+ * (min(x,y) = y<x ? y : x, max(x,y) = x<y ? y : x). GLSL's pow has no fixed
+ * rounding, so the friction's h^(-4/3) is evaluated by the kernels'
+ * division-free Newton sequence (inv_pow43 below), and sqrt(g h) as
+ * sqrt(g) sqrt(h): values the reference admits, bit-identical to the
  * product's.
  *
  * One deliberate choice: the GLSL source kernel reads a neighbour's depth
@@ -105,14 +109,18 @@ static inline float gclamp(float x, float lo, float hi) { return gmin(gmax(x, lo
    same expressions as the CUDA kernels. */
 static const float ONE_THIRD = 1.0f / 3.0f;
 
-/* x^(1/3) for x > 0 by Newton's iteration r <- (2r + x/r^2) * (1/3) from the
-   bit-level estimate bits(x)/3 + (2/3)*127*2^23 (the exponent divided by
-   three), then x * r. Basic IEEE operations only. */
-static float pow43(float x) {
-    uint32_t i = fbits(x);
-    float r = bitsf(i / 3u + 0x2A555555u);
-    for (int k = 0; k < 4; ++k) r = (2.0f * r + x / (r * r)) * ONE_THIRD;
-    return x * r;
+/* x^(-4/3) for x > 0 without a division: y = x^(-1/3) by Newton's iteration
+   for 1/y^3 = x, y <- y + (y/3)(1 - x y^3), from the exponent-thirds estimate
+   bits(y) = (4/3)*127*2^23 - bits(x)/3, four steps; then (y^2)^2. Multiplies
+   and fused multiply-adds only. */
+static float inv_pow43(float x) {
+    float y = bitsf(0x54AAAAAAu - fbits(x) / 3u);
+    for (int k = 0; k < 4; ++k) {
+        float t = x * (y * y);
+        y = fmaf(y * ONE_THIRD, fmaf(-t, y, 1.0f), y);
+    }
+    float y2 = y * y;
+    return y2 * y2;
 }
 
 static float safe_vel(const oracle_t *o, float h_, float hq) {
@@ -135,12 +143,13 @@ static void safe_vel2(const oracle_t *o, float h_, float hq1, float hq2, float *
 
 static void hllc_speeds(const oracle_t *o, float hL, float unL, float hR, float unR, float *SLo, float *SRo) {
     float g = o->g;
-    float cL = sqrtf(g * gmax(hL, 0.0f));
-    float cR = sqrtf(g * gmax(hR, 0.0f));
     float sqL = sqrtf(gmax(hL, 0.0f));
     float sqR = sqrtf(gmax(hR, 0.0f));
+    float root_g = sqrtf(g);
+    float cL = root_g * sqL;
+    float cR = root_g * sqR;
     float den = sqL + sqR;
-    float u_roe = (den > 1e-12f) ? (sqL * unL + sqR * unR) / den : 0.0f;
+    float u_roe = (den > 1e-12f) ? fmaf(sqL, unL, sqR * unR) / den : 0.0f;
     float c_roe = sqrtf(g * 0.5f * (hL + hR));
     float SL = gmin(unL - cL, u_roe - c_roe);
     float SR = gmax(unR + cR, u_roe + c_roe);
@@ -149,8 +158,8 @@ static void hllc_speeds(const oracle_t *o, float hL, float unL, float hR, float 
     float dryLeft = (1.0f - wetL) * wetR;
     float dryRight = (1.0f - wetR) * wetL;
     float roe = 1.0f - dryLeft - dryRight;
-    *SLo = roe * SL + dryLeft * (unR - 2.0f * cR) + dryRight * (unL - cL);
-    *SRo = roe * SR + dryLeft * (unR + cR) + dryRight * (unL + 2.0f * cL);
+    *SLo = fmaf(roe, SL, fmaf(dryLeft, fmaf(-2.0f, cR, unR), dryRight * (unL - cL)));
+    *SRo = fmaf(roe, SR, fmaf(dryLeft, unR + cR, dryRight * fmaf(2.0f, cL, unL)));
 }
 
 static void hllc(const oracle_t *o, float hL, float hqnL, float hqtL, float hR, float hqnR, float hqtR,
@@ -162,24 +171,25 @@ static void hllc(const oracle_t *o, float hL, float hqnL, float hqtL, float hR, 
     float SL, SR;
     hllc_speeds(o, hL, unL, hR, unR, &SL, &SR);
     *Smax = gmax(fabsf(SL), fabsf(SR));
-    float num_sm = SL * hR * (unR - SR) - SR * hL * (unL - SL);
-    float den_sm = hR * (unR - SR) - hL * (unL - SL);
+    float aR = hR * (unR - SR), aL = hL * (unL - SL);
+    float num_sm = fmaf(SL, aR, -(SR * aL));
+    float den_sm = aR - aL;
     float SM = (fabsf(den_sm) > 1e-12f) ? num_sm / den_sm : 0.0f;
     float FL_h = hL * unL;
-    float FL_hn = hL * unL * unL + 0.5f * g * hL * hL;
-    float FL_ht = hL * unL * utL;
+    float FL_hn = fmaf(FL_h, unL, 0.5f * g * hL * hL);
+    float FL_ht = FL_h * utL;
     float FR_h = hR * unR;
-    float FR_hn = hR * unR * unR + 0.5f * g * hR * hR;
-    float FR_ht = hR * unR * utR;
+    float FR_hn = fmaf(FR_h, unR, 0.5f * g * hR * hR);
+    float FR_ht = FR_h * utR;
     float dSL = SL - SM, dSR = SR - SM;
     float kL = hL * (SL - unL) / ((fabsf(dSL) > 1e-14f) ? dSL : 1e-14f);
     float kR = hR * (SR - unR) / ((fabsf(dSR) > 1e-14f) ? dSR : 1e-14f);
-    float FsL_h = FL_h + SL * (kL - hL);
-    float FsL_hn = FL_hn + SL * (kL * SM - hL * unL);
-    float FsL_ht = FL_ht + SL * (kL * utL - hL * utL);
-    float FsR_h = FR_h + SR * (kR - hR);
-    float FsR_hn = FR_hn + SR * (kR * SM - hR * unR);
-    float FsR_ht = FR_ht + SR * (kR * utR - hR * utR);
+    float FsL_h = fmaf(SL, kL - hL, FL_h);
+    float FsL_hn = fmaf(SL, fmaf(kL, SM, -FL_h), FL_hn);
+    float FsL_ht = fmaf(SL, (kL - hL) * utL, FL_ht);
+    float FsR_h = fmaf(SR, kR - hR, FR_h);
+    float FsR_hn = fmaf(SR, fmaf(kR, SM, -FR_h), FR_hn);
+    float FsR_ht = fmaf(SR, (kR - hR) * utR, FR_ht);
     if (SL >= 0.0f) { *Fh = FL_h; *Fhn = FL_hn; *Fht = FL_ht; }
     else if (SM >= 0.0f) { *Fh = FsL_h; *Fhn = FsL_hn; *Fht = FsL_ht; }
     else if (SR >= 0.0f) { *Fh = FsR_h; *Fhn = FsR_hn; *Fht = FsR_ht; }
@@ -195,10 +205,10 @@ static void face_states(const oracle_t *o, float hL, float huL, float hvL, float
     safe_vel2(o, hL, huL, hvL, &uL, &vL);
     safe_vel2(o, hR, huR, hvR, &uR, &vR);
     float huLs = *hLs * uL, hvLs = *hLs * vL, huRs = *hRs * uR, hvRs = *hRs * vR;
-    *hqnL = huLs * nx_ + hvLs * ny_;
-    *hqtL = -huLs * ny_ + hvLs * nx_;
-    *hqnR = huRs * nx_ + hvRs * ny_;
-    *hqtR = -huRs * ny_ + hvRs * nx_;
+    *hqnL = fmaf(huLs, nx_, hvLs * ny_);
+    *hqtL = fmaf(hvLs, nx_, -(huLs * ny_));
+    *hqnR = fmaf(huRs, nx_, hvRs * ny_);
+    *hqtR = fmaf(hvRs, nx_, -(huRs * ny_));
 }
 
 static float wave_bound(const oracle_t *o, float hL, float huL, float hvL, float dzL, float hR, float huR,
@@ -344,8 +354,9 @@ void oracle_flux_stage(oracle_t *o, int stage) {
             load_state(o, stage, cL, &hL, &huL, &hvL);
             if (cR == -1) {
                 hR = hL;
-                huR = huL - 2.0f * (huL * nx_ + hvL * ny_) * nx_;
-                hvR = hvL - 2.0f * (huL * nx_ + hvL * ny_) * ny_;
+                float twice = -2.0f * fmaf(huL, nx_, hvL * ny_);
+                huR = fmaf(twice, nx_, huL);
+                hvR = fmaf(twice, ny_, hvL);
             } else if (cR < 0) {
                 ghost_state(o, open_kind(o, cR), open_value(o, cR), hL, huL, hvL, nx_, ny_, &hR, &huR, &hvR);
             } else {
@@ -371,18 +382,18 @@ void oracle_flux_stage(oracle_t *o, int stage) {
             } else if (cR < 0) {
                 Fh = 0.0f; /* a wall passes no mass */
             }
-            float Fhu = Fhn * nx_ - Fht * ny_;
-            float Fhv = Fhn * ny_ + Fht * nx_;
-            float SL_g = 0.5f * o->g * (hL * hL - hLs * hLs);
-            float SR_g = 0.5f * o->g * (hR * hR - hRs * hRs);
+            float Fhu = fmaf(Fhn, nx_, -(Fht * ny_));
+            float Fhv = fmaf(Fhn, ny_, Fht * nx_);
+            float SL_g = 0.5f * o->g * fmaf(hL, hL, -(hLs * hLs));
+            float SR_g = 0.5f * o->g * fmaf(hR, hR, -(hRs * hRs));
             o->touched[cL] = 1u;
             if (cR >= 0) o->touched[cR] = 1u;
             float *w = o->ef + EF_WORDS * eid;
             w[0] = Fh * len;
-            w[1] = Fhu * len + SL_g * nx_ * len;
-            w[2] = Fhv * len + SL_g * ny_ * len;
-            w[3] = Fhu * len + SR_g * nx_ * len;
-            w[4] = Fhv * len + SR_g * ny_ * len;
+            w[1] = fmaf(SL_g, nx_, Fhu) * len;
+            w[2] = fmaf(SL_g, ny_, Fhv) * len;
+            w[3] = fmaf(SR_g, nx_, Fhu) * len;
+            w[4] = fmaf(SR_g, ny_, Fhv) * len;
             if (stage) w[EF_CFL] = Smax * len;
         }
     }
@@ -453,8 +464,8 @@ void oracle_update_stage(oracle_t *o, int stage, int compensated, int track_clam
             h_new = gmax(h_raw, 0.0f);
             lo_new = 0.0f;
         }
-        float hu_new = hui - dti * sdhu;
-        float hv_new = hvi - dti * sdhv;
+        float hu_new = fmaf(-dti, sdhu, hui);
+        float hv_new = fmaf(-dti, sdhv, hvi);
         if (track_clamp) o->clamp_mass[i] += 0.5f * A * (h_new - h_raw);
         if (h_new < o->dry_tol) { hu_new = 0.0f; hv_new = 0.0f; }
         if (h_new >= o->dry_tol) {
@@ -466,10 +477,9 @@ void oracle_update_stage(oracle_t *o, int stage, int compensated, int track_clam
             float n = o->n_mann[i];
             float inv_h = 1.0f / h_new;
             float u_ = hu_new * inv_h, v_ = hv_new * inv_h;
-            float spd = sqrtf(u_ * u_ + v_ * v_);
-            float h43 = pow43(h_new);
-            float Sf = o->g * n * n * spd / h43;
-            float inv_den = 1.0f / (1.0f + dt * Sf);
+            float spd = sqrtf(fmaf(u_, u_, v_ * v_));
+            float Sf = o->g * n * n * spd * inv_pow43(h_new);
+            float inv_den = 1.0f / fmaf(dt, Sf, 1.0f);
             hu_new = hu_new * inv_den;
             hv_new = hv_new * inv_den;
         }
@@ -647,7 +657,7 @@ void oracle_step(oracle_t *o, const uint32_t *src_cells, const float *src_rate, 
     oracle_step_control(o->ctrl, o->dt_buf, 1);
 }
 
-float oracle_pow43(float x) { return pow43(x); }
+float oracle_inv_pow43(float x) { return inv_pow43(x); }
 
 void oracle_hllc(float g, float dry_tol, const float *in6, float *out4) {
     oracle_t o;

@@ -87,8 +87,8 @@ def lib() -> ctypes.CDLL:
     global _LIB
     if _LIB is None:
         _LIB = ctypes.CDLL(str(build()))
-        _LIB.oracle_pow43.restype = ctypes.c_float
-        _LIB.oracle_pow43.argtypes = [ctypes.c_float]
+        _LIB.oracle_inv_pow43.restype = ctypes.c_float
+        _LIB.oracle_inv_pow43.argtypes = [ctypes.c_float]
         _LIB.oracle_sizeof.restype = ctypes.c_size_t
         _LIB.oracle_ctrl_sizeof.restype = ctypes.c_size_t
     return _LIB
@@ -390,8 +390,9 @@ class ResidentOracle:
             self.open_volume_snapshots.append(self.download_open_volumes())
 
 
-def pow43(x: float) -> float:
-    return float(lib().oracle_pow43(ctypes.c_float(x)))
+def inv_pow43(x: float) -> float:
+    """x^(-4/3) as the kernels evaluate it (the friction slope's depth power)."""
+    return float(lib().oracle_inv_pow43(ctypes.c_float(x)))
 
 
 def step_control(ctrl: np.ndarray, dt_buf: np.ndarray, mode: int) -> None:
