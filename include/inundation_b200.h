@@ -326,9 +326,12 @@ int swe_volume_fp64(const float *h, const float *h_lo, const float *area, uint32
    a static 8 KiB device array that every GPU loading this library holds until
    exit, so n_cells is limited to 4,194,304 (SWE_ERR_TOO_LARGE above). Call it
    with the stream's device current; its first call on a device looks up the
-   array's address, so make that first call before any stream capture. All
-   calls share the array: calls that overlap on the GPU (other streams, other
-   threads) race and must be serialised by the caller. */
+   array's address, so make that first call before any stream capture. The
+   address is kept for the life of the process: after a cudaDeviceReset the
+   module may load elsewhere, so a process that resets a device must not call
+   this entry point on that device again. All calls share the array: calls
+   that overlap on the GPU (other streams, other threads) race and must be
+   serialised by the caller. */
 int swe_volume_fp64_noalloc(const float *h, const float *h_lo, const float *area, uint32_t n_cells, double *out,
                             swe_stream_t stream);
 

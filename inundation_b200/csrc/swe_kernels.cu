@@ -184,7 +184,8 @@ extern "C" int swe_volume_fp64_noalloc(const float *h, const float *h_lo, const 
     double *scratch = g_volume_scratch_addr[dev].load(std::memory_order_acquire);
     if (scratch == nullptr) {
         // First call on this device (the device must be current): look up the
-        // array's device address once and keep it.
+        // array's device address once and keep it for the life of the process
+        // (a cudaDeviceReset may load the module elsewhere: see the header).
         void *addr = nullptr;
         if (cudaGetSymbolAddress(&addr, g_volume_scratch) != cudaSuccess || addr == nullptr) return SWE_ERR_CUDA;
         scratch = static_cast<double *>(addr);
