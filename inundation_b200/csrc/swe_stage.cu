@@ -50,9 +50,11 @@ inline size_t block_smem_bytes(uint32_t max_tile_edges) {
 // sdhv at sums[i], sums[n + i], sums[2n + i], n = padded cells), the record
 // the adjoint reverses. OPEN: the mesh has open edges.
 // ---------------------------------------------------------------------------
-// CTAs of the block kernel that must fit on one SM (registers per thread follow from it).
+// CTAs of the block kernel that must fit on one SM: 8 x 256 threads caps a thread at 32
+// registers, so the SM holds its full 64 warps; the measured all-wet step is fastest there
+// (fewer registers and CTAs cost more than the few spilled words).
 #ifndef SWE_BLOCK_MIN_CTAS
-#define SWE_BLOCK_MIN_CTAS 1
+#define SWE_BLOCK_MIN_CTAS 8
 #endif
 
 template <int STAGE, bool COMP, bool CLAMP, bool OPEN>
