@@ -645,7 +645,8 @@ def run_whole_hour(sc, args, device: str) -> dict:
             "steps": n,
             "wall_s": recs[-1].wall_s - prev_wall,
             "active_fraction": c / (g.N * n) if n else 0.0,
-            "active_blocks_at_end": recs[-1].active_blocks / solver.n_blocks,
+            "active_blocks_max": max(r.active_blocks for r in recs if r.steps) / solver.n_blocks
+            if any(r.steps for r in recs) else 0.0,
             "kernel_steps": kernels,
         })
         prev_wall, prev_computed = recs[-1].wall_s, recs[-1].computed_cells
@@ -761,6 +762,8 @@ def finish_error_by_horizon(fut, region, states, dts, reach) -> dict:
             "hu_max_abs": float(np.abs(hu[region.cells] - hu64).max()),
             "hv_max_abs": float(np.abs(hv[region.cells] - hv64).max()),
             "h_rms_wet_m": float(np.sqrt(np.mean((h[region.cells] - h64)[h64 > 0] ** 2))) if (h64 > 0).any() else 0.0,
+            "h_p999_abs_m": float(np.quantile(np.abs(h[region.cells] - h64)[h64 > 0], 0.999)) if (h64 > 0).any() else 0.0,
+            "cells_over_tolerance": int((np.abs(h[region.cells] - h64) > 1e-5).sum()),
             "wet_cells": int((h64 > 0).sum()),
             "oracle_rim_max_h_m": rim,
             "cuda_max_h_outside_m": float(np.abs(h[outside]).max()) if outside.any() else 0.0,

@@ -93,6 +93,81 @@ __device__ __forceinline__ void update_cell(const swe_state_t &s, const Phys &p,
     if (lam > 1e-30f && A > 1e-10f) bound = __float_as_uint(cfl * A / lam);
 }
 
+// The edge flux with the two sides of every symmetric step in the two lanes of a
+// float2 (lane x the left side, lane y the right): Blackwell's paired float32
+// instructions (__fadd2_rn, __fmul2_rn, __ffma2_rn) round each lane exactly as
+// the scalar operation would, so face_flux_pair gives the values of face_states +
+// hllc (swe_math.cuh) bit for bit, in fewer instructions. A difference x - y is
+// written x + (-y) or fma(-1, y, x), which round to the same value.
+__device__ __forceinline__ float2 pr(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+// safe_vel2 of both sides: the velocities of momenta q1, q2 at depth h, per lane.
+__device__ __forceinline__ void safe_vel_pair(const Phys &p, float2 h, float2 q1, float2 q2, float2 &v1, float2 &v2) {
+    const float e = kFilmDepths * p.dry_tol;
+    const float2 hh = mul2(h, h);
+    const float2 den = add2(hh, pr(gmax(hh.x, e * e), gmax(hh.y, e * e)));
+    const float2 inv = pr(1.0f / den.x, 1.0f / den.y);
+    const float2 twice = mul2(pr(2.0f, 2.0f), h);
+    v1 = mul2(mul2(twice, q1), inv);
+    v2 = mul2(mul2(twice, q2), inv);
+    if (!(h.x > p.dry_tol)) v1.x = v2.x = 0.0f;
+    if (!(h.y > p.dry_tol)) v1.y = v2.y = 0.0f;
+}
+
+// face_states + hllc: the reconstructed depths hs and the face-frame HLLC flux and speed bound.
+__device__ __forceinline__ void face_flux_pair(const Phys &p, float nx, float ny, float2 dz, float2 h, float2 hu,
+                                               float2 hv, float2 &hs, float &Fh, float &Fhn, float &Fht,
+                                               float &smax) {
+    const float2 dh = add2(h, pr(-dz.x, -dz.y));
+    hs = pr(gmax(0.0f, dh.x), gmax(0.0f, dh.y));
+    float2 u, v;
+    safe_vel_pair(p, h, hu, hv, u, v);
+    const float2 hus = mul2(hs, u), hvs = mul2(hs, v);
+    const float2 qn = fma2(hus, pr(nx, nx), mul2(hvs, pr(ny, ny)));
+    const float2 qt = fma2(hvs, pr(nx, nx), mul2(hus, pr(-ny, -ny)));
+    float2 un, ut;
+    safe_vel_pair(p, hs, qn, qt, un, ut);
+    const float sqL = sqrtf(gmax(hs.x, 0.0f)), sqR = sqrtf(gmax(hs.y, 0.0f));
+    const float root_g = sqrtf(p.g);
+    const float2 c = mul2(pr(root_g, root_g), pr(sqL, sqR));
+    const float den = sqL + sqR;
+    const float u_roe = (den > 1e-12f) ? fmaf_rn(sqL, un.x, sqR * un.y) / den : 0.0f;
+    const float c_roe = sqrtf(p.g * 0.5f * (hs.x + hs.y));
+    const float2 a = fma2(pr(-1.0f, 1.0f), c, un);
+    const float2 b = fma2(pr(-1.0f, 1.0f), pr(c_roe, c_roe), pr(u_roe, u_roe));
+    const float SL0 = gmin(a.x, b.x), SR0 = gmax(a.y, b.y);
+    const float wetL = wet_blend(p, hs.x), wetR = wet_blend(p, hs.y);
+    const float2 dry = mul2(add2(pr(1.0f, 1.0f), pr(-wetL, -wetR)), pr(wetR, wetL));
+    const float roe = 1.0f - dry.x - dry.y;
+    const float2 m1 = fma2(pr(-2.0f, 1.0f), pr(c.y, c.y), pr(un.y, un.y));
+    const float2 m2 = fma2(pr(-1.0f, 2.0f), pr(c.x, c.x), pr(un.x, un.x));
+    const float2 S = fma2(pr(roe, roe), pr(SL0, SR0), fma2(pr(dry.x, dry.x), m1, mul2(pr(dry.y, dry.y), m2)));
+    const float SL = S.x, SR = S.y;
+    smax = gmax(fabsf(SL), fabsf(SR));
+    const float2 aRL = mul2(pr(hs.y, hs.x), add2(pr(un.y, un.x), pr(-SR, -SL)));
+    const float num_sm = fmaf_rn(SL, aRL.x, -(SR * aRL.y));
+    const float den_sm = aRL.x - aRL.y;
+    const float SM = (fabsf(den_sm) > 1e-12f) ? num_sm / den_sm : 0.0f;
+    const bool left = (SL >= 0.0f) || (SM >= 0.0f);
+    const bool star = !(SL >= 0.0f) && (left || SR >= 0.0f);
+    const float hX = left ? hs.x : hs.y, unX = left ? un.x : un.y, utX = left ? ut.x : ut.y;
+    const float q = hX * unX;
+    Fh = q;
+    Fhn = fmaf_rn(q, unX, 0.5f * p.g * hX * hX);
+    Fht = q * utX;
+    if (star) {
+        const float Sx = left ? SL : SR;
+        const float dS = Sx - SM;
+        const float k = hX * (Sx - unX) / ((fabsf(dS) > 1e-14f) ? dS : 1e-14f);
+        Fh = fmaf_rn(Sx, k - hX, q);
+        Fhn = fmaf_rn(Sx, fmaf_rn(k, SM, -q), Fhn);
+        Fht = fmaf_rn(Sx, (k - hX) * utX, Fht);
+    }
+}
+
 // Flux of one edge from its two cell states: the five gather words and the
 // corrector's CFL word (resident.py:254-284). On an open edge (cR < -1,
 // condition kind/value) the mass flux follows the condition, and an
@@ -103,14 +178,13 @@ __device__ __forceinline__ void edge_words(const Phys &p, int cR, float nx, floa
                                            float dzR, float hL, float huL, float hvL, float hR, float huR,
                                            float hvR, float &w0, float &w1, float &w2, float &w3, float &w4,
                                            float &w5, uint32_t kind = kOpenWall, float value = 0.0f) {
-    float hLs, hqnL, hqtL, hRs, hqnR, hqtR, Fh, Fhn, Fht, smax;
-    face_states(p, hL, huL, hvL, dzL, hR, huR, hvR, dzR, nx, ny, hLs, hqnL, hqtL, hRs, hqnR, hqtR);
-    hllc(p, hLs, hqnL, hqtL, hRs, hqnR, hqtR, Fh, Fhn, Fht, smax);
+    float2 hs;
+    float Fh, Fhn, Fht, smax;
+    face_flux_pair(p, nx, ny, pr(dzL, dzR), pr(hL, hR), pr(huL, huR), pr(hvL, hvR), hs, Fh, Fhn, Fht, smax);
     if (OPEN && cR < -1) {
         if ((kind == kOpenFree || kind == kOpenNormal) && Fh < 0.0f) {
             ghost_state(p, kOpenWall, 0.0f, hL, huL, hvL, nx, ny, hR, huR, hvR);
-            face_states(p, hL, huL, hvL, dzL, hR, huR, hvR, dzR, nx, ny, hLs, hqnL, hqtL, hRs, hqnR, hqtR);
-            hllc(p, hLs, hqnL, hqtL, hRs, hqnR, hqtR, Fh, Fhn, Fht, smax);
+            face_flux_pair(p, nx, ny, pr(dzL, dzR), pr(hL, hR), pr(huL, huR), pr(hvL, hvR), hs, Fh, Fhn, Fht, smax);
             Fh = 0.0f;
         } else {
             Fh = boundary_mass_flux(kind, value, Fh);
@@ -118,15 +192,16 @@ __device__ __forceinline__ void edge_words(const Phys &p, int cR, float nx, floa
     } else if (cR < 0) {
         Fh = 0.0f;  // a wall passes no mass
     }
-    const float Fhu = fmaf_rn(Fhn, nx, -(Fht * ny));
-    const float Fhv = fmaf_rn(Fhn, ny, Fht * nx);
-    const float SL_g = 0.5f * p.g * fmaf_rn(hL, hL, -(hLs * hLs));
-    const float SR_g = 0.5f * p.g * fmaf_rn(hR, hR, -(hRs * hRs));
+    const float2 F = fma2(pr(Fhn, Fhn), pr(nx, ny), mul2(pr(Fht, Fht), pr(-ny, nx)));
+    const float2 hs2 = mul2(hs, hs);
+    const float2 hyd = mul2(pr(0.5f * p.g, 0.5f * p.g), fma2(pr(hL, hR), pr(hL, hR), pr(-hs2.x, -hs2.y)));
+    const float2 wn = mul2(fma2(hyd, pr(nx, nx), pr(F.x, F.x)), pr(len, len));
+    const float2 wt = mul2(fma2(hyd, pr(ny, ny), pr(F.y, F.y)), pr(len, len));
     w0 = Fh * len;
-    w1 = fmaf_rn(SL_g, nx, Fhu) * len;
-    w2 = fmaf_rn(SL_g, ny, Fhv) * len;
-    w3 = fmaf_rn(SR_g, nx, Fhu) * len;
-    w4 = fmaf_rn(SR_g, ny, Fhv) * len;
+    w1 = wn.x;
+    w2 = wt.x;
+    w3 = wn.y;
+    w4 = wt.y;
     w5 = smax * len;
 }
 // ---------------------------------------------------------------------------
