@@ -210,7 +210,7 @@ template <bool COMP, bool CLAMP, bool OPEN>
 __device__ bool seat_predictor(const swe_mesh_t &m, const swe_state_t &s, const Phys &p, float cfl,
                                unsigned char *smem, TiledShared<kPersistThreads> &sh, SeatShared &ss, uint32_t *ph,
                                uint64_t &computed, uint32_t step, uint32_t epoch, bool all_active, bool sources) {
-    const TilePlan L = tile_plan(m.max_sub_edges, m.max_sub_slots, kTileCols);
+    const TilePlan L = tile_plan(m.max_sub_edges, m.max_sub_slots, 10u);
     float *F = reinterpret_cast<float *>(smem + L.total);
     const TileBuf B0 = tile_buf(smem, L, 0u), B1 = tile_buf(smem, L, 1u);
     const uint32_t tid = threadIdx.x;
@@ -349,7 +349,7 @@ template <bool COMP, bool CLAMP, bool OPEN>
 __device__ bool seat_corrector(const swe_mesh_t &m, const swe_state_t &s, const Phys &p, float cfl,
                                unsigned char *smem, TiledShared<kPersistThreads> &sh, SeatShared &ss, uint32_t *ph,
                                uint64_t &computed, uint32_t step, uint32_t epoch, bool all_active) {
-    const TilePlan L = tile_plan(m.max_sub_edges, m.max_sub_slots, kTileCols);
+    const TilePlan L = tile_plan(m.max_sub_edges, m.max_sub_slots, 10u);
     float *F = reinterpret_cast<float *>(smem + L.total);
     const TileBuf B0 = tile_buf(smem, L, 0u), B1 = tile_buf(smem, L, 1u);
     const uint32_t tid = threadIdx.x, next = epoch + 1u, qpar = (step + 1u) & 1u;

@@ -39,17 +39,9 @@ __device__ __forceinline__ TileSmem tile_smem(uint32_t cap) {
     return t;
 }
 
-// The block kernel's staged cells after the edge words: depth and velocity (u, v) of the
-// block's 256 cells, each computed once per stage instead of once per edge end.
 inline size_t block_smem_bytes(uint32_t max_tile_edges) {
     const size_t cap = (max_tile_edges + 3u) & ~3u;
-    return cap * 6 * sizeof(float) + ((cap + 15) & ~size_t(15)) + 3u * kBlockCells * sizeof(float);
-}
-
-__device__ __forceinline__ float *block_cell_smem(uint32_t cap) {
-    extern __shared__ float4 smem4[];
-    return reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(smem4) + cap * 6 * sizeof(float) +
-                                     ((cap + 15) & ~15u));
+    return cap * 6 * sizeof(float) + ((cap + 15) & ~size_t(15));
 }
 
 // ---------------------------------------------------------------------------
@@ -70,7 +62,6 @@ __global__ void __launch_bounds__(kThreads, SWE_BLOCK_MIN_CTAS)
     stage_block_kernel(swe_mesh_t m, swe_state_t s, Phys p, float cfl, float *sums) {
     const uint32_t cap = (m.max_tile_edges + 3u) & ~3u;
     const TileSmem t = tile_smem(cap);
-    float *const cell_h = block_cell_smem(cap), *const cell_u = cell_h + kBlockCells, *const cell_v = cell_u + kBlockCells;
     __shared__ uint32_t red[kThreads / 32];
     const uint32_t count = s.sched[kSchedActive];
     uint64_t computed = 0;
@@ -82,68 +73,24 @@ __global__ void __launch_bounds__(kThreads, SWE_BLOCK_MIN_CTAS)
         if (dt_bits == 0u) continue;  // this instance's window is done: a no-op step
         const float dt = __uint_as_float(dt_bits);
         const uint32_t base = m.tile_ptr[b], ne = m.tile_count[b], cells = m.block_cells[b];
-        const uint32_t c0 = b * kBlockCells, i = c0 + threadIdx.x;
-
-        // The block's cells: the stage's input state (the predictor in the corrector: the
-        // block is active) and its velocities, staged once for every edge that ends here.
-        if (threadIdx.x < cells) {
-            const float hi = STAGE ? s.h1[i] : s.h[i];
-            const float hui = STAGE ? s.hu1[i] : s.hu[i];
-            const float hvi = STAGE ? s.hv1[i] : s.hv[i];
-            float ui, vi;
-            safe_vel2(p, hi, hui, hvi, ui, vi);
-            cell_h[threadIdx.x] = hi;
-            cell_u[threadIdx.x] = ui;
-            cell_v[threadIdx.x] = vi;
-        }
-        __syncthreads();
 
         for (uint32_t j = threadIdx.x; j < ne; j += kThreads) {
             const uint32_t e = base + j;
             const int cL = m.tile_cl[e], cR = m.tile_cr[e];
             const float nx = m.tile_nx[e], ny = m.tile_ny[e];
-            const uint32_t lL = static_cast<uint32_t>(cL) - c0;
-            if (cR >= 0) {
-                // an interior edge: depths and velocities, staged or from the neighbouring block
-                float hL, uL, vL, hR, uR, vR;
-                if (lL < static_cast<uint32_t>(kBlockCells)) {
-                    hL = cell_h[lL];
-                    uL = cell_u[lL];
-                    vL = cell_v[lL];
-                } else {
-                    float huL, hvL;
-                    load_state<STAGE>(s, cL, hL, huL, hvL);
-                    safe_vel2(p, hL, huL, hvL, uL, vL);
-                }
-                const uint32_t lR = static_cast<uint32_t>(cR) - c0;
-                if (lR < static_cast<uint32_t>(kBlockCells)) {
-                    hR = cell_h[lR];
-                    uR = cell_u[lR];
-                    vR = cell_v[lR];
-                } else {
-                    float huR, hvR;
-                    load_state<STAGE>(s, cR, hR, huR, hvR);
-                    safe_vel2(p, hR, huR, hvR, uR, vR);
-                }
-                const bool live = !(hL < p.dry_tol && hR < p.dry_tol);
-                t.live[j] = live;
-                if (!live) continue;
-                float c;
-                interior_words(p, nx, ny, m.tile_len[e], m.tile_dzl[e], m.tile_dzr[e], hL, uL, vL, hR, uR, vR,
-                               t.F0[j], t.L1[j], t.L2[j], t.R1[j], t.R2[j], c);
-                if (STAGE == 1) t.C[j] = c;
-                continue;
-            }
-            // a wall or an open edge of a cell of this block: its ghost needs the momenta
             float hL, huL, hvL, hR, huR, hvR;
             load_state<STAGE>(s, cL, hL, huL, hvL);
             uint32_t kind = kOpenWall;
             float value = 0.0f;
-            if (OPEN) {
-                boundary_state(m, p, cR, hL, huL, hvL, nx, ny, hR, huR, hvR, kind, value);
+            if (cR < 0) {
+                if (OPEN) {
+                    boundary_state(m, p, cR, hL, huL, hvL, nx, ny, hR, huR, hvR, kind, value);
+                } else {
+                    hR = hL;
+                    wall_mirror(huL, hvL, nx, ny, huR, hvR);
+                }
             } else {
-                hR = hL;
-                wall_mirror(huL, hvL, nx, ny, huR, hvR);
+                load_state<STAGE>(s, cR, hR, huR, hvR);
             }
             const bool live = !(hL < p.dry_tol && hR < p.dry_tol) || (OPEN && open_forced(kind, value));
             t.live[j] = live;
@@ -156,6 +103,7 @@ __global__ void __launch_bounds__(kThreads, SWE_BLOCK_MIN_CTAS)
         }
         __syncthreads();
 
+        const uint32_t i = b * kBlockCells + threadIdx.x;
         bool wet = false;
         uint32_t bound = kNoBound;
         if (threadIdx.x < cells) {
@@ -175,7 +123,7 @@ __global__ void __launch_bounds__(kThreads, SWE_BLOCK_MIN_CTAS)
                 }
                 if (STAGE == 1) lam += t.C[j];
             }
-            const float hi = cell_h[threadIdx.x], hui = STAGE ? s.hu1[i] : s.hu[i];
+            const float hi = STAGE ? s.h1[i] : s.h[i], hui = STAGE ? s.hu1[i] : s.hu[i];
             const float hvi = STAGE ? s.hv1[i] : s.hv[i];
             const float loi = COMP ? (STAGE ? s.h1_lo[i] : s.h_lo[i]) : 0.0f;
             const float h0 = STAGE ? s.h[i] : 0.0f, hu0 = STAGE ? s.hu[i] : 0.0f, hv0 = STAGE ? s.hv[i] : 0.0f;
@@ -242,7 +190,7 @@ int launch_stage(const swe_mesh_t *m, const swe_state_t *s, const swe_params_t *
         return check_launch();
     }
     auto kern = stage_tiled_kernel<STAGE, COMP, CLAMP, OPEN>;
-    const size_t bytes = tile_plan(m->max_sub_edges, m->max_sub_slots, kTileCols).total;
+    const size_t bytes = tile_plan(m->max_sub_edges, m->max_sub_slots, STAGE ? 10u : 6u).total;
     int rc = set_smem(kern, bytes);
     if (rc) return rc;
     kern<<<p->grid ? p->grid : 148u * 8u, kTileThreads, bytes, st>>>(*m, *s, ph, p->cfl, sums);
@@ -268,7 +216,7 @@ int dispatch_stage(const swe_mesh_t *m, const swe_state_t *s, const swe_params_t
 template <int STAGE, bool COMP, bool CLAMP>
 int configure_stage(const swe_mesh_t *m) {
     const size_t block = block_smem_bytes(m->max_tile_edges);
-    const size_t tiled = tile_plan(m->max_sub_edges, m->max_sub_slots, kTileCols).total;
+    const size_t tiled = tile_plan(m->max_sub_edges, m->max_sub_slots, STAGE ? 10u : 6u).total;
     int rc = set_smem(stage_block_kernel<STAGE, COMP, CLAMP, false>, block);
     if (!rc) rc = set_smem(stage_block_kernel<STAGE, COMP, CLAMP, true>, block);
     if (!rc) rc = set_smem(stage_tiled_kernel<STAGE, COMP, CLAMP, false>, tiled);
@@ -301,7 +249,7 @@ int swe_configure(const swe_mesh_t *mesh, int kernel, int *blocks_per_sm) {
     if (kernel == 0) {
         err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
             blocks_per_sm, stage_tiled_kernel<1, true, false, false>, kTileThreads,
-            tile_plan(mesh->max_sub_edges, mesh->max_sub_slots, kTileCols).total);
+            tile_plan(mesh->max_sub_edges, mesh->max_sub_slots, 10u).total);
     } else {
         err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, stage_block_kernel<1, true, false, false>, kThreads,
                                                             block_smem_bytes(mesh->max_tile_edges));

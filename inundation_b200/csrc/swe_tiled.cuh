@@ -118,12 +118,13 @@ __device__ __forceinline__ void safe_vel_pair(const Phys &p, float2 h, float2 q1
 }
 
 // face_states + hllc: the reconstructed depths hs and the face-frame HLLC flux and speed bound.
-// The same from the two cells' velocities (u, v), their safe_vel2 values, computed beforehand.
-__device__ __forceinline__ void face_flux_pair_vel(const Phys &p, float nx, float ny, float2 dz, float2 h, float2 u,
-                                                   float2 v, float2 &hs, float &Fh, float &Fhn, float &Fht,
-                                                   float &smax) {
+__device__ __forceinline__ void face_flux_pair(const Phys &p, float nx, float ny, float2 dz, float2 h, float2 hu,
+                                               float2 hv, float2 &hs, float &Fh, float &Fhn, float &Fht,
+                                               float &smax) {
     const float2 dh = add2(h, pr(-dz.x, -dz.y));
     hs = pr(gmax(0.0f, dh.x), gmax(0.0f, dh.y));
+    float2 u, v;
+    safe_vel_pair(p, h, hu, hv, u, v);
     const float2 hus = mul2(hs, u), hvs = mul2(hs, v);
     const float2 qn = fma2(hus, pr(nx, nx), mul2(hvs, pr(ny, ny)));
     const float2 qt = fma2(hvs, pr(nx, nx), mul2(hus, pr(-ny, -ny)));
@@ -167,42 +168,6 @@ __device__ __forceinline__ void face_flux_pair_vel(const Phys &p, float nx, floa
     }
 }
 
-// face_states + hllc: the reconstructed depths hs and the face-frame HLLC flux and speed bound.
-__device__ __forceinline__ void face_flux_pair(const Phys &p, float nx, float ny, float2 dz, float2 h, float2 hu,
-                                               float2 hv, float2 &hs, float &Fh, float &Fhn, float &Fht,
-                                               float &smax) {
-    float2 u, v;
-    safe_vel_pair(p, h, hu, hv, u, v);
-    face_flux_pair_vel(p, nx, ny, dz, h, u, v, hs, Fh, Fhn, Fht, smax);
-}
-
-// The gather words of an edge from the reconstruction's depths and the face-frame flux.
-__device__ __forceinline__ void flux_words(const Phys &p, float nx, float ny, float len, float hL, float hR, float2 hs,
-                                           float Fh, float Fhn, float Fht, float smax, float &w0, float &w1,
-                                           float &w2, float &w3, float &w4, float &w5) {
-    const float2 F = fma2(pr(Fhn, Fhn), pr(nx, ny), mul2(pr(Fht, Fht), pr(-ny, nx)));  // (Fhu, Fhv)
-    const float2 hs2 = mul2(hs, hs);
-    const float2 hyd = mul2(pr(0.5f * p.g, 0.5f * p.g), fma2(pr(hL, hR), pr(hL, hR), pr(-hs2.x, -hs2.y)));
-    const float2 wn = mul2(fma2(hyd, pr(nx, nx), pr(F.x, F.x)), pr(len, len));  // (w1, w3)
-    const float2 wt = mul2(fma2(hyd, pr(ny, ny), pr(F.y, F.y)), pr(len, len));  // (w2, w4)
-    w0 = Fh * len;
-    w1 = wn.x;
-    w2 = wt.x;
-    w3 = wn.y;
-    w4 = wt.y;
-    w5 = smax * len;
-}
-
-// edge_words of an interior edge (both cells real) from the cells' depths and velocities.
-__device__ __forceinline__ void interior_words(const Phys &p, float nx, float ny, float len, float dzL, float dzR,
-                                               float hL, float uL, float vL, float hR, float uR, float vR, float &w0,
-                                               float &w1, float &w2, float &w3, float &w4, float &w5) {
-    float2 hs;
-    float Fh, Fhn, Fht, smax;
-    face_flux_pair_vel(p, nx, ny, pr(dzL, dzR), pr(hL, hR), pr(uL, uR), pr(vL, vR), hs, Fh, Fhn, Fht, smax);
-    flux_words(p, nx, ny, len, hL, hR, hs, Fh, Fhn, Fht, smax, w0, w1, w2, w3, w4, w5);
-}
-
 // Flux of one edge from its two cell states: the five gather words and the
 // corrector's CFL word (resident.py:254-284). On an open edge (cR < -1,
 // condition kind/value) the mass flux follows the condition, and an
@@ -227,7 +192,17 @@ __device__ __forceinline__ void edge_words(const Phys &p, int cR, float nx, floa
     } else if (cR < 0) {
         Fh = 0.0f;  // a wall passes no mass
     }
-    flux_words(p, nx, ny, len, hL, hR, hs, Fh, Fhn, Fht, smax, w0, w1, w2, w3, w4, w5);
+    const float2 F = fma2(pr(Fhn, Fhn), pr(nx, ny), mul2(pr(Fht, Fht), pr(-ny, nx)));
+    const float2 hs2 = mul2(hs, hs);
+    const float2 hyd = mul2(pr(0.5f * p.g, 0.5f * p.g), fma2(pr(hL, hR), pr(hL, hR), pr(-hs2.x, -hs2.y)));
+    const float2 wn = mul2(fma2(hyd, pr(nx, nx), pr(F.x, F.x)), pr(len, len));
+    const float2 wt = mul2(fma2(hyd, pr(ny, ny), pr(F.y, F.y)), pr(len, len));
+    w0 = Fh * len;
+    w1 = wn.x;
+    w2 = wt.x;
+    w3 = wn.y;
+    w4 = wt.y;
+    w5 = smax * len;
 }
 // ---------------------------------------------------------------------------
 // 64-cell tiles from work items, staged by bulk copies.
@@ -235,12 +210,6 @@ __device__ __forceinline__ void edge_words(const Phys &p, int cR, float nx, floa
 struct TilePlan {
     uint32_t capE, capS, nc, buf_bytes, total;
 };
-
-// Columns of 64 floats in a staged buffer: [0..3] the stage's input state, [4] area,
-// [5] n, [6..9] the committed state (stage 1) or the kept state of the persistent
-// kernel, [10, 11] the velocities the tile computes from its input state.
-constexpr uint32_t kTileVelCol = 10u;
-constexpr uint32_t kTileCols = 12u;
 
 __host__ __device__ inline TilePlan tile_plan(uint32_t max_edges, uint32_t max_slots, uint32_t nc) {
     TilePlan L;
@@ -255,7 +224,7 @@ __host__ __device__ inline TilePlan tile_plan(uint32_t max_edges, uint32_t max_s
 struct TileBuf {
     int32_t *cl, *cr;
     float *nx, *ny, *len, *dzl, *dzr;
-    float *c;        // nc x 64: the columns of kTileCols
+    float *c;        // nc x 64: [0..3] the stage's input state, [4] area, [5] n, [6..9] committed state (stage 1)
     uint32_t *cptr;  // 68
     uint16_t *lcsr;
     uint64_t *bar;
@@ -362,7 +331,7 @@ struct LateDt {
 // persistent kernel, whose buffers keep their records from step to step) the
 // flux words in arrays of their own (7 per record).
 __host__ __device__ inline size_t tiled_smem_bytes(uint32_t max_edges, uint32_t max_slots, bool keep) {
-    const TilePlan L = tile_plan(max_edges, max_slots, kTileCols);
+    const TilePlan L = tile_plan(max_edges, max_slots, 10u);
     return keep ? L.total + 7u * L.capE * 4u : L.total;
 }
 
@@ -395,52 +364,10 @@ __device__ __forceinline__ bool tile_compute(const swe_mesh_t &m, const swe_stat
     float *W3 = F ? F + 4 * capE : B.dzl, *W4 = F ? F + 5 * capE : B.dzr;
     int32_t *W5 = F ? reinterpret_cast<int32_t *>(F + 6 * capE) : B.cl;
 
-    // The tile's cell velocities, once per stage (columns kTileVelCol, kTileVelCol + 1).
-    float *const U = B.c + kTileVelCol * kTileCells, *const V = U + kTileCells;
-    if (tid < it.cells) safe_vel2(p, C0[tid], C1[tid], C2[tid], U[tid], V[tid]);
-    __syncthreads();
-
     // Edge fluxes.
     for (uint32_t j = tid; j < it.ne; j += TPB) {
         const int cL = B.cl[j], cR = B.cr[j];
         const float nx = B.nx[j], ny = B.ny[j];
-        if (cR >= 0) {
-            // an interior edge: depths and velocities, staged or from a neighbouring tile
-            float hL, uL, vL, hR, uR, vR;
-            const uint32_t lL = static_cast<uint32_t>(cL - base), lR = static_cast<uint32_t>(cR - base);
-            if (lL < static_cast<uint32_t>(kTileCells)) {
-                hL = C0[lL];
-                uL = U[lL];
-                vL = V[lL];
-            } else {
-                float huL, hvL;
-                load_state<STAGE>(s, cL, hL, huL, hvL);
-                safe_vel2(p, hL, huL, hvL, uL, vL);
-            }
-            if (lR < static_cast<uint32_t>(kTileCells)) {
-                hR = C0[lR];
-                uR = U[lR];
-                vR = V[lR];
-            } else {
-                float huR, hvR;
-                load_state<STAGE>(s, cR, hR, huR, hvR);
-                safe_vel2(p, hR, huR, hvR, uR, vR);
-            }
-            const bool live = !(hL < p.dry_tol && hR < p.dry_tol);
-            const float len = B.len[j], dzl = B.dzl[j], dzr = B.dzr[j];
-            live_w[j] = live ? 1 : 0;
-            if (!live) continue;
-            float w0, w1, w2, w3, w4, w5;
-            interior_words(p, nx, ny, len, dzl, dzr, hL, uL, vL, hR, uR, vR, w0, w1, w2, w3, w4, w5);
-            W0[j] = w0;
-            W1[j] = w1;
-            W2[j] = w2;
-            W3[j] = w3;
-            W4[j] = w4;
-            if (STAGE == 1) W5[j] = __float_as_int(w5);
-            continue;
-        }
-        // a wall or an open edge: its ghost needs the momenta of the cell inside
         float hL, huL, hvL, hR, huR, hvR;
         const uint32_t lL = static_cast<uint32_t>(cL - base);
         if (lL < static_cast<uint32_t>(kTileCells)) {
@@ -452,11 +379,22 @@ __device__ __forceinline__ bool tile_compute(const swe_mesh_t &m, const swe_stat
         }
         uint32_t kind = kOpenWall;
         float value = 0.0f;
-        if (OPEN) {
-            boundary_state(m, p, cR, hL, huL, hvL, nx, ny, hR, huR, hvR, kind, value);
+        if (cR < 0) {
+            if (OPEN) {
+                boundary_state(m, p, cR, hL, huL, hvL, nx, ny, hR, huR, hvR, kind, value);
+            } else {
+                hR = hL;
+                wall_mirror(huL, hvL, nx, ny, huR, hvR);
+            }
         } else {
-            hR = hL;
-            wall_mirror(huL, hvL, nx, ny, huR, hvR);
+            const uint32_t lR = static_cast<uint32_t>(cR - base);
+            if (lR < static_cast<uint32_t>(kTileCells)) {
+                hR = C0[lR];
+                huR = C1[lR];
+                hvR = C2[lR];
+            } else {
+                load_state<STAGE>(s, cR, hR, huR, hvR);
+            }
         }
         const bool live = !(hL < p.dry_tol && hR < p.dry_tol) || (OPEN && open_forced(kind, value));
         const float len = B.len[j], dzl = B.dzl[j], dzr = B.dzr[j];
@@ -543,7 +481,8 @@ __device__ __forceinline__ bool tile_compute(const swe_mesh_t &m, const swe_stat
 template <int STAGE, bool COMP, bool CLAMP, int TPB, bool OPEN>
 __device__ bool tiled_pass(const swe_mesh_t &m, const swe_state_t &s, const Phys &p, float cfl, unsigned char *smem,
                            TiledShared<TPB> &sh, uint32_t &k, uint64_t &computed, float *sums = nullptr) {
-    const TilePlan L = tile_plan(m.max_sub_edges, m.max_sub_slots, kTileCols);
+    constexpr uint32_t nc = STAGE ? 10u : 6u;
+    const TilePlan L = tile_plan(m.max_sub_edges, m.max_sub_slots, nc);
     uint32_t *red = sh.red;
     uint4 *items = sh.items;
     uint32_t *dts = sh.dts;
