@@ -94,6 +94,9 @@ def parse_args() -> argparse.Namespace:
                     help="only check the adjoint at 250k cells against float64 central differences and print that")
     ap.add_argument("--fd-steps", type=int, default=200, help="--adjoint-fd: steps of the checked run")
     ap.add_argument("--fd-directions", type=int, default=20, help="--adjoint-fd: random directions")
+    ap.add_argument("--fd-eps", default="1e-2,3e-3",
+                    help="--adjoint-fd: the two step sizes of the central differences (a direction counts as smooth "
+                         "where they agree)")
     args = ap.parse_args()
     cells, seed = WORKLOADS[args.workload]
     args.cells = cells if args.cells is None else args.cells
@@ -1222,8 +1225,9 @@ def adjoint_fd_check(args, local: int) -> dict:
 
     * directional derivatives along ``--fd-directions`` seeded random directions of (n, z, q)
       by central differences of the float64 loss (the same discrete step in float64 on the GPU,
-      ``oracle/torch_step.py``, with the CUDA run's dt frozen), at two step sizes, the
-      direction counted as smooth where they agree to 1e-3;
+      ``oracle/torch_step.py``, with the CUDA run's dt frozen), at the two step sizes of
+      ``--fd-eps``, the direction counted as smooth where they agree to 1e-2 (with wetting fronts
+      the loss has kinks: too small a step measures them instead of the slope);
     * the CUDA gradient (derivatives cut below the film depth, 4 dry_tol) against those
       differences of the exact loss: the cut surrogate's bias and the float32 error together;
     * float64 autograd with the same cut against the same differences (the bias alone) and
@@ -1269,6 +1273,7 @@ def adjoint_fd_check(args, local: int) -> dict:
     loss_cut.backward()
     an, az, aq = (v.grad.cpu().numpy() for v in (n_t, z_t, q_t))
     n0, z0, q0 = (np.asarray(v, np.float64) for v in (n, z, q))
+    eps_a, eps_b = (float(v) for v in args.fd_eps.split(","))
     rows = []
     with torch.no_grad():
         base = float(loss64(exact, t64(n0), t64(z0), t64(q0)))
@@ -1283,7 +1288,7 @@ def adjoint_fd_check(args, local: int) -> dict:
             dn = rng.standard_normal(n0.size) * 0.005
             dz = rng.standard_normal(z0.size) * 0.01
             dq = rng.standard_normal(q0.size) * 2.0
-            d1, d2 = fd(dn, dz, dq, 1e-5), fd(dn, dz, dq, 2e-6)
+            d1, d2 = fd(dn, dz, dq, eps_a), fd(dn, dz, dq, eps_b)
             cuda = (float(np.dot(gn, dn)), float(np.dot(gz, dz)), float(np.dot(gq, dq)))
             ref = (float(np.dot(an, dn)), float(np.dot(az, dz)), float(np.dot(aq, dq)))
             scale = sum(abs(v) for v in cuda)
@@ -1291,7 +1296,7 @@ def adjoint_fd_check(args, local: int) -> dict:
                 "direction": k,
                 "fd": d1,
                 "fd_fine": d2,
-                "smooth": abs(d1 - d2) <= 1e-3 * max(abs(d1), 1e-300),
+                "smooth": abs(d1 - d2) <= 1e-2 * max(abs(d1), 1e-300),
                 "cuda_cut": sum(cuda),
                 "f64_cut": sum(ref),
                 "err_cuda_cut_vs_fd": abs(sum(cuda) - d1) / scale,
@@ -1329,8 +1334,9 @@ def adjoint_fd_check(args, local: int) -> dict:
         },
         "rows": rows,
         "wall_s": time.perf_counter() - t_all,
+        "fd_eps": [eps_a, eps_b],
         "reference": "float64 torch restatement of the same discrete step on the GPU (oracle/torch_step.py), dt "
-        "frozen at the CUDA run's values; central differences at eps 1e-5 and 2e-6 of the exact (uncut) loss",
+        "frozen at the CUDA run's values; central differences of the exact (uncut) loss",
     }
 
 

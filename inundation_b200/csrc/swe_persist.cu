@@ -353,6 +353,9 @@ __device__ bool seat_corrector(const swe_mesh_t &m, const swe_state_t &s, const 
     float *F = reinterpret_cast<float *>(smem + L.total);
     const TileBuf B0 = tile_buf(smem, L, 0u), B1 = tile_buf(smem, L, 1u);
     const uint32_t tid = threadIdx.x, next = epoch + 1u, qpar = (step + 1u) & 1u;
+    const uint32_t n = ss.n_extra;
+    // the first other tile's restaging flies while the seat computes (buffer 1 is free)
+    if (n && tid < 32u) seat_issue<1>(m, s, ss.extra[0], B1, false);
     if (ss.seat_active) {
         const Item it = unpack(ss.seat_item);
         const bool wet = tile_compute<1, COMP, CLAMP, kPersistThreads, OPEN>(
@@ -365,9 +368,8 @@ __device__ bool seat_corrector(const swe_mesh_t &m, const swe_state_t &s, const 
         fence_proxy_async();
         __syncthreads();
     }
-    const uint32_t n = ss.n_extra;
     for (uint32_t w = 0; w < n; ++w) {
-        if (tid < 32u) seat_issue<1>(m, s, ss.extra[w], B1, false);
+        if (w > 0u && tid < 32u) seat_issue<1>(m, s, ss.extra[w], B1, false);
         if (!seat_wait(s, B1, ph, 1u)) return false;
         const Item it = unpack(ss.extra[w]);
         const bool wet = tile_compute<1, COMP, CLAMP, kPersistThreads, OPEN>(
