@@ -134,41 +134,44 @@ __device__ __forceinline__ uint64_t ld_relaxed_u64(const uint64_t *p) {
     asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
-__device__ __forceinline__ void st_release_u64(uint64_t *p, uint64_t v) {
-    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+__device__ __forceinline__ void st_relaxed_u64(uint64_t *p, uint64_t v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
 // -- integer-tick step control (resident.py:813-885) ---------------------------------------------
 __device__ __forceinline__ uint32_t step_control(swe_ctrl_t *c, uint32_t *dt_buf, int mode) {
-    float raw;
+    // Every input is read before anything is written, so all the loads are in flight at
+    // once (one round trip: this runs on the critical path of the persistent kernel).
+    const uint64_t now0 = c->now_ticks, stop = c->stop_ticks, steps0 = c->steps;
+    const uint32_t done = c->dt_ticks, dt_max = c->dt_max_ticks, dry_dt = c->dry_dt_ticks;
+    const float last0 = c->last_raw, safety = c->cfl_safety;
+    const uint32_t bound0 = dt_buf[0], bound1 = dt_buf[1];
+    uint64_t now = now0, steps = steps0;
+    float raw = last0;  // a no-op step computed no bound; RETARGET replans from the last one
     if (mode == 0) {
-        raw = __uint_as_float(dt_buf[0]);
-        c->last_raw = raw;
+        raw = __uint_as_float(bound0);
     } else if (mode == 1) {
-        const uint32_t done = c->dt_ticks;
-        c->now_ticks += static_cast<uint64_t>(done);
+        now += static_cast<uint64_t>(done);
         if (done > 0u) {
-            c->steps += 1u;
-            raw = __uint_as_float(dt_buf[1]);
-            c->last_raw = raw;
-        } else {
-            raw = c->last_raw;  // a no-op step computed no bound
+            steps += 1u;
+            raw = __uint_as_float(bound1);
         }
-    } else {
-        raw = c->last_raw;
     }
-    const uint64_t remaining = (c->stop_ticks > c->now_ticks) ? c->stop_ticks - c->now_ticks : 0ull;
+    const uint64_t remaining = (stop > now) ? stop - now : 0ull;
     uint32_t ticks;
     if (remaining == 0ull || raw < 1e-10f || raw != raw) {
         ticks = 0u;  // window done, or a degenerate bound: the host sees no progress
     } else if (raw >= 1e10f) {
-        ticks = c->dry_dt_ticks;  // no wet edge anywhere
+        ticks = dry_dt;  // no wet edge anywhere
     } else {
-        const float cap = static_cast<float>(c->dt_max_ticks) / kTicksPerSecond;
-        ticks = static_cast<uint32_t>(gmin(raw * c->cfl_safety, cap) * kTicksPerSecond);
+        const float cap = static_cast<float>(dt_max) / kTicksPerSecond;
+        ticks = static_cast<uint32_t>(gmin(raw * safety, cap) * kTicksPerSecond);
     }
-    if (c->dt_max_ticks < ticks) ticks = c->dt_max_ticks;
+    if (dt_max < ticks) ticks = dt_max;
     if (static_cast<uint64_t>(ticks) > remaining) ticks = static_cast<uint32_t>(remaining);
+    c->now_ticks = now;
+    c->steps = steps;
+    c->last_raw = raw;
     c->dt_ticks = ticks;
     const uint32_t dt = __float_as_uint(static_cast<float>(ticks) / kTicksPerSecond);
     dt_buf[0] = dt;

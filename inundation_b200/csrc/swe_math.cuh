@@ -196,8 +196,9 @@ __device__ __forceinline__ void wall_mirror(float huL, float hvL, float nx, floa
 constexpr uint32_t kOpenWall = 0u, kOpenFree = 1u, kOpenNormal = 2u, kOpenStage = 3u, kOpenInflow = 4u;
 constexpr int kOpenNewtonSteps = 4;
 
-// Cube root of x >= 0 by the Newton iteration of pow43 (no fixed-rounding pow is
-// assumed; this is one value GLSL's pow(x, 1/3) admits).
+// Cube root of x >= 0 by Newton's iteration r <- (2r + x/r^2)/3 from the exponent-thirds
+// estimate, four steps (no fixed-rounding pow is assumed; this is one value GLSL's
+// pow(x, 1/3) admits).
 __device__ __forceinline__ float cbrt_newton(float x) {
     if (!(x > 0.0f)) return 0.0f;
     float r = __uint_as_float(__float_as_uint(x) / 3u + 0x2A555555u);

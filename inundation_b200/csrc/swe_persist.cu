@@ -177,7 +177,7 @@ __device__ __forceinline__ void seat_take(const swe_mesh_t &m, const swe_state_t
                                           uint32_t epoch, bool all_active) {
     if (threadIdx.x == 0) {
         uint32_t got = kNoTile;
-        for (;;) {
+        for (; ss.qlen != 0u;) {  // an empty queue needs no round trip to find so
             uint32_t *taken = step == 0u ? &s.sched[kSchedStartTaken] : &s.sched[kSchedQCons + (step & 1u)];
             const uint32_t idx = atomicAdd(taken, 1u);
             if (idx >= ss.qlen) break;
@@ -224,14 +224,15 @@ __device__ bool seat_predictor(const swe_mesh_t &m, const swe_state_t &s, const 
             if (tid < 32u) seat_issue<0>(m, s, ss.seat_item, B0, true);
             if (!seat_wait(s, B0, ph, 0u)) return false;
         }
-        const LateDt late{dt_pair(s, it.inst), s.marks + 2u * b, epoch, all_active ? 1u : 0u, sh.late};
+        // the queue's length (final since the last barrier) arrives with them
+        const LateDt late{dt_pair(s, it.inst), s.marks + 2u * b, s.sched + kSchedQProd + (step & 1u), epoch,
+                          all_active ? 1u : 0u, sh.late};
         tile_compute<0, COMP, CLAMP, kPersistThreads, OPEN>(m, s, p, cfl, B0, it, 0.0f, 0u, 6u, F, L.capE, sh.red,
                                                             computed, true, nullptr, &late);
         fence_proxy_async();
         if (tid == 0) {
             ss.n_extra = 0u;
-            ss.qlen = step == 0u ? *reinterpret_cast<volatile uint32_t *>(s.sched + kSchedItems)
-                                 : *reinterpret_cast<volatile uint32_t *>(s.sched + kSchedQProd + (step & 1u));
+            ss.qlen = sh.late[2];
             const uint32_t dt = sh.late[1];
             ss.seat_active = sh.late[0] != 0u ? 1u : 0u;
             ss.seat_dt = sh.late[0];
@@ -492,7 +493,8 @@ __global__ void __launch_bounds__(kPersistThreads, 1024 / kPersistThreads)
         auto control = [&] {
             for (uint32_t i = threadIdx.x; i < m.n_inst; i += blockDim.x) {
                 const uint32_t dt = step_control(s.ctrl + i, s.dt_buf + kDtWords * i, 1);
-                st_release_u64(const_cast<uint64_t *>(dt_pair(s, i)), (static_cast<uint64_t>(next_epoch) << 32) | dt);
+                // readers use the pair's own 64 bits only: no release ordering to wait for
+                st_relaxed_u64(const_cast<uint64_t *>(dt_pair(s, i)), (static_cast<uint64_t>(next_epoch) << 32) | dt);
             }
             if (threadIdx.x == blockDim.x - 1u) {  // beside instance 0's control, not after it
                 volatile uint32_t *sched = s.sched;

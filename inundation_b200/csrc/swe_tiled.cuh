@@ -306,7 +306,7 @@ __device__ __forceinline__ void tile_issue(const swe_mesh_t &m, const swe_state_
 // Shared words of a tile pass besides the staged buffers.
 template <int TPB>
 struct TiledShared {
-    uint32_t late[2];  // LateDt's slot
+    uint32_t late[3];  // LateDt's slots
     uint32_t red[TPB / 32];
     uint4 items[2];
     uint32_t dts[2];
@@ -322,9 +322,10 @@ struct TiledShared {
 struct LateDt {
     const uint64_t *dt;    // the instance's published (dt, epoch) pair
     const uint32_t *mark;  // the block's epoch word
+    const uint32_t *queue; // a word read beside them (the length of this step's tile queue)
     uint32_t epoch;        // this step's epoch: of an active block, and of the pair
     uint32_t all;          // every block is active
-    uint32_t *slot;        // two shared words
+    uint32_t *slot;        // three shared words: dt if active (else 0), dt, the queue word
 };
 
 // Shared-memory bytes of a tile pass: two staged buffers, and with `keep` (the
@@ -351,10 +352,11 @@ __device__ __forceinline__ bool tile_compute(const swe_mesh_t &m, const swe_stat
     const uint32_t tid = threadIdx.x;
     const uint32_t b = it.tile >> 2;
     uint64_t late_pair = 0u;
-    uint32_t late_mark = 0u;
+    uint32_t late_mark = 0u, late_queue = 0u;
     if (late && tid == 0) {  // in flight while the fluxes are computed
         late_pair = ld_relaxed_u64(late->dt);
         late_mark = *late->mark;
+        late_queue = *reinterpret_cast<const volatile uint32_t *>(late->queue);
     }
     if (STAGE == 0 && !late && (it.tile & 3u) == 0u && tid == 0) s.blk[kBlkWords * b + kBlkWet] = 0u;
     const float *C0 = B.c + in_col * kTileCells, *C1 = C0 + kTileCells, *C2 = C0 + 2 * kTileCells;
@@ -416,6 +418,7 @@ __device__ __forceinline__ bool tile_compute(const swe_mesh_t &m, const swe_stat
         const bool active = late->all || late_mark == late->epoch;
         late->slot[0] = active ? late_dt : 0u;
         late->slot[1] = late_dt;
+        late->slot[2] = late_queue;
         if (STAGE == 0 && active && late_dt != 0u && (it.tile & 3u) == 0u) s.blk[kBlkWords * b + kBlkWet] = 0u;
     }
     __syncthreads();

@@ -250,8 +250,9 @@ static void add_compensated(float hi, float loi, float inc, float *h_new, float 
 #define OPEN_INFLOW 4u
 #define OPEN_NEWTON_STEPS 4
 
-/* x^(1/3) for x >= 0 by pow43's Newton sequence: GLSL's pow(x, 1/3) has no
-   fixed rounding, and this is a value it admits. */
+/* x^(1/3) for x >= 0 by Newton's iteration r <- (2r + x/r^2)/3 from the
+   exponent-thirds estimate, four steps: GLSL's pow(x, 1/3) has no fixed
+   rounding, and this is a value it admits. */
 static float cbrt_newton(float x) {
     if (!(x > 0.0f)) return 0.0f;
     float r = bitsf(fbits(x) / 3u + 0x2A555555u);
