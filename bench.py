@@ -75,7 +75,7 @@ def parse_args() -> argparse.Namespace:
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--chunk", type=int, default=500, help="steps per captured graph in the timed region")
-    ap.add_argument("--kernel", choices=["auto", "tiled", "plain", "persistent"], default="auto",
+    ap.add_argument("--kernel", choices=["auto", "tiled", "plain", "staged", "persistent"], default="auto",
                     help="stage kernel variant (auto: by the active fraction after the prologue)")
     ap.add_argument("--ctas-per-sm", type=int, default=None, help="persistent CTAs per SM of the stage kernel")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-scenarios measurement")
@@ -883,7 +883,7 @@ def run_sources_workload(args, world: int, rank: int, local: int, built=None) ->
         per_cell = json.loads(tfile.read_text()).get(kernel, {}).get("dram_bytes_per_computed_cell_step")
         if per_cell:
             traffic = per_cell * computed / stage_launches
-    per_step_launches = {"persistent": 0, "plain": 5, "tiled": 5}[kernel]  # stages, sources (2), dilation
+    per_step_launches = {"persistent": 0, "plain": 5, "staged": 5, "tiled": 5}[kernel]  # stages, sources (2), dilation
 
     # End to end through the public calls: the spun-up state from host arrays, a clock restart, the
     # same number of steps (the timed region's graphs, already captured), the final depth back.

@@ -56,8 +56,10 @@ typedef struct {
    rest pad an instance to whole blocks). Its 256-cell tile is the contiguous
    range [tile_ptr[b], tile_ptr[b + 1]) of the tile_* arrays, tile_count[b]
    records then padding to a multiple of 32: first the edges whose left cell
-   is in b (the reference's resident edge order, gpu_resident_batch.py:175),
-   then the edges whose right cell is in b and left cell is not.
+   is in b and right cell in b or a boundary, then those whose left cell is in
+   b and right cell in another block, then the edges whose right cell is in b
+   and left cell is not, each group in the reference's resident edge order
+   (gpu_resident_batch.py:175).
    lcsr[k] = (position in the tile << 1) | is_right for the CSR slots k of each
    cell, in the reference's per-cell order (inundation/mesh/geometry.py:454-468,
    remapped as blocks.py:33-44).
@@ -108,6 +110,13 @@ typedef struct {
        cell's bed, or the discharge per unit width). NULL when n_open is 0. */
     uint32_t n_open;
     const uint32_t *open_cond;
+    /* The local CSR of the 256-cell tiles regrouped per tile like sub_lcsr: tile b's
+       slots from blk_lcsr[blk_lcsr_ptr[b]] (multiples of 8), the array 8 slots longer than
+       its last segment; max_blk_slots the longest segment. Read by stage kernel 3 only
+       (may be NULL otherwise). */
+    uint32_t max_blk_slots;
+    const uint16_t *blk_lcsr;
+    const uint32_t *blk_lcsr_ptr; /* n_blocks + 1 */
 } swe_mesh_t;
 
 /* Mutable state and the run workspace (device pointers). */
@@ -150,7 +159,8 @@ typedef struct {
     uint32_t kernel;      /* stage kernel: 0 = 64-cell tiles staged by bulk copies (default),
                              1 = 256-cell blocks with plain loads,
                              2 = swe_steps only: whole steps of 64-cell tiles in one persistent cooperative
-                                 launch, phases separated by bounded grid barriers */
+                                 launch, phases separated by bounded grid barriers,
+                             3 = 256-cell blocks staged by bulk copies (needs blk_lcsr) */
 } swe_params_t;
 
 /* Sparse sources (device pointers), one per cell: source k adds
@@ -172,7 +182,7 @@ typedef struct {
     uint32_t n_hydro;
 } swe_sources_t;
 
-/* n_steps whole steps: swe_step n_steps times (kernel 0 or 1), or one persistent cooperative launch
+/* n_steps whole steps: swe_step n_steps times (kernel 0, 1 or 3), or one persistent cooperative launch
    running them all (kernel 2; params->grid caps its CTAs, 0 = as many as fit; status 3 when
    (4 n_steps + 1) x CTAs reaches 2^32, the range of its barrier counter). A wait of the
    persistent kernel that times out records error 2 in the control block. */
@@ -290,7 +300,7 @@ typedef struct {
 int swe_bed_steps(const swe_mesh_t *mesh, const float *z, float *tile_dzl, float *tile_dzr, uint32_t tile_records,
                   float *sub_dzl, float *sub_dzr, uint32_t sub_records, swe_stream_t stream);
 
-/* swe_stage (kernel 0 or 1) that also stores every computed cell's gathered sums. */
+/* swe_stage (kernel 0, 1 or 3) that also stores every computed cell's gathered sums. */
 int swe_stage_taped(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params_t *params, int stage,
                     float *sums, swe_stream_t stream);
 

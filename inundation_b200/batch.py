@@ -260,7 +260,7 @@ def autotune(
         solver.stage_kernel, solver.ctas_per_sm = best["stage_kernel"], best["ctas_per_sm"]
         return best
     if candidates is None:
-        candidates = [(k, c) for k in ("tiled", "plain", "persistent") for c in (None, 4, 2)]
+        candidates = [(k, c) for k in ("tiled", "plain", "staged", "persistent") for c in (None, 4, 2)]
     saved_spg = solver.steps_per_graph
     results = []
     for kernel, per_sm in candidates:

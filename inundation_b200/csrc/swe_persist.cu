@@ -592,10 +592,10 @@ using namespace swe;
 
 extern "C" int swe_steps(const swe_mesh_t *mesh, const swe_state_t *state, const swe_params_t *params,
                          const swe_sources_t *sources, uint32_t n_steps, swe_stream_t stream) {
-    if (!mesh_ok(mesh) || !state_ok(state) || !open_ok(mesh, state) || !params || !sources || params->kernel > 2u)
+    if (!mesh_ok(mesh) || !state_ok(state) || !open_ok(mesh, state) || !params || !sources || params->kernel > 3u)
         return SWE_ERR_ARGUMENT;
     if (n_steps == 0u) return SWE_OK;
-    if (params->kernel < 2u) {
+    if (params->kernel != 2u) {
         for (uint32_t k = 0; k < n_steps; ++k) {
             const int rc = swe_step(mesh, state, params, sources, stream);
             if (rc) return rc;

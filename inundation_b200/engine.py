@@ -44,7 +44,7 @@ RESIDENT_CTRL_DTYPE = np.dtype(
 
 START, STEP, RETARGET = 0, 1, 2
 STATE_ARRAYS = ("h", "hu", "hv", "h_lo", "h1", "hu1", "hv1", "h1_lo", "clamp_mass")
-KERNELS = {"tiled": 0, "plain": 1, "persistent": 2}
+KERNELS = {"tiled": 0, "plain": 1, "persistent": 2, "staged": 3}
 # "auto": the persistent kernel while few blocks are active (its phases are latency-bound), the
 # 256-cell block kernel once more than this fraction of blocks is active (issue-bound work), unless
 # every active tile still has a CTA of the persistent grid to itself (a small mesh).
@@ -84,7 +84,8 @@ class ResidentEngine:
     track_clamp: bool = False
     cfl_safety: float = 1.0
     # Stage kernel: "tiled" (64-cell tiles from the dilation's work items, staged by bulk copies),
-    # "plain" (256-cell blocks, direct loads), "persistent" (the tiled stages and the rest of the
+    # "plain" (256-cell blocks, direct loads), "staged" (256-cell blocks staged by bulk copies),
+    # "persistent" (the tiled stages and the rest of the
     # step in one cooperative launch per submit, phases separated by grid barriers) or "auto"
     # (persistent or plain by the active fraction read after every submit). All give the same bits.
     stage_kernel: str = "auto"
@@ -137,6 +138,8 @@ class ResidentEngine:
         t["lcsr"] = self._dev(B.lcsr.view(np.int16))
         t["sub_lcsr"] = self._dev(S.lcsr_blk.view(np.int16))
         t["sub_lcsr_ptr"] = self._dev(_i32(S.lcsr_ptr))
+        t["blk_lcsr"] = self._dev(B.lcsr_blk.view(np.int16))
+        t["blk_lcsr_ptr"] = self._dev(_i32(B.lcsr_ptr))
         self.n_open = L.n_open
         if L.n_open:  # conditions start as walls; the pointer stays fixed, so graphs see every update
             t["open_cond"] = torch.zeros(2 * L.n_open, dtype=torch.int32, device=self.device)
@@ -148,6 +151,7 @@ class ResidentEngine:
         m.n_inst = L.n_inst
         m.max_sub_edges = S.max_edges
         m.max_sub_slots = S.max_slots
+        m.max_blk_slots = B.max_slots
         for name, tensor in t.items():
             setattr(m, name, tensor.data_ptr())
         m.n_open = L.n_open
@@ -166,7 +170,7 @@ class ResidentEngine:
         """Persistent CTAs of a stage kernel: CTAs per SM x SMs, at most one per work unit."""
         kernel = self._kernel if kernel is None else kernel
         per_sm = self._per_sm[kernel] if self.ctas_per_sm is None else min(self.ctas_per_sm, self._per_sm[kernel])
-        units = self.n_blocks if kernel == 1 else 4 * self.n_blocks  # 64-cell tiles, or 256-cell blocks
+        units = self.n_blocks if kernel in (1, 3) else 4 * self.n_blocks  # 256-cell blocks, or 64-cell tiles
         grid = min(units, per_sm * self._sms)
         if self.max_grid is not None:
             grid = min(grid, self.max_grid)

@@ -6,10 +6,13 @@ stably by the 256-cell block of the left cell,
 tile ``t`` is cells ``[T t, T t + T)`` and owns one contiguous segment of edge
 records, structure-of-arrays:
 
-* the edges whose left cell is in the tile, in resident order, then
-* the edges whose right cell is in the tile and left cell is not, in resident
-  order,
+* the edges whose left cell is in the tile and whose right cell is in it too
+  (or is a boundary), then
+* the edges whose left cell is in the tile and right cell in another tile, then
+* the edges whose right cell is in the tile and left cell is not,
 
+each group in resident order, so the records that read another tile's state
+come last and fill the last warps of a tile pass,
 padded to a multiple of ``TILE_ALIGN`` records so every segment starts on a
 128-byte boundary of every array. One CTA then finds, in one segment, every
 edge its cells touch. ``lcsr`` replaces the reference's remapped CSR
@@ -112,7 +115,10 @@ def _tile_set(geom: MeshGeometry, order: NDArray[np.int64], signed: NDArray[np.i
     t_l = ecl // tile_cells
     t_r = np.where(ecr >= 0, ecr // tile_cells, -1)
 
-    own_sorted = np.argsort(t_l, kind="stable")
+    # a tile's own edges whose right cell lies in another tile go after the others: the records
+    # that read state from outside the tile sit together at the segment's end
+    outside = (t_r >= 0) & (t_r != t_l)
+    own_sorted = np.lexsort((np.arange(n_e), outside, t_l))
     n_own = np.bincount(t_l, minlength=n_t)
     own_first = np.zeros(n_t + 1, dtype=np.int64)
     np.cumsum(n_own, out=own_first[1:])

@@ -69,6 +69,9 @@ class SweMesh(ctypes.Structure):
         )],
         ("n_open", _U32),
         ("open_cond", _P),
+        ("max_blk_slots", _U32),
+        ("blk_lcsr", _P),
+        ("blk_lcsr_ptr", _P),
     ]
 
 

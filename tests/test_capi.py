@@ -91,8 +91,10 @@ def test_whole_steps_refuse_a_misaligned_dt_buffer(lib: ctypes.CDLL) -> None:
 
 
 def test_ctypes_structs_match_the_header_layout() -> None:
-    assert ctypes.sizeof(native.SweMesh) == 16 + 17 * 8 + 8 + 11 * 8 + 8 + 8  # n_open (padded), open_cond
+    # ... n_open (padded), open_cond, max_blk_slots (padded), blk_lcsr, blk_lcsr_ptr
+    assert ctypes.sizeof(native.SweMesh) == 16 + 17 * 8 + 8 + 11 * 8 + 8 + 8 + 8 + 8 + 8
     assert native.SweMesh.n_open.offset == 248 and native.SweMesh.open_cond.offset == 256
+    assert native.SweMesh.max_blk_slots.offset == 264 and native.SweMesh.blk_lcsr_ptr.offset == 280
     assert ctypes.sizeof(native.SweState) == 18 * 8
     assert ctypes.sizeof(native.SweParams) == 32
     assert ctypes.sizeof(native.SweSources) == 7 * 8 + 8

@@ -71,7 +71,7 @@ def batch_case():
     return solver, ms
 
 
-@pytest.mark.parametrize("kernel", ["tiled", "plain", "persistent"])
+@pytest.mark.parametrize("kernel", ["tiled", "plain", "staged", "persistent"])
 def test_every_instance_matches_its_own_oracle_run(kernel: str, batch_case) -> None:
     solver, ms = batch_case
     solver.stage_kernel = kernel
@@ -142,10 +142,10 @@ def test_fixed_step_runs_and_autotuner_keep_results() -> None:
         m.h0 = np.where(np.arange(m.geom.N) < m.geom.N // 5, 0.3, 0.0).astype(np.float32)
     solver = BatchedSolver(ms)
     choice = autotune(solver, dt_max=1.0, dt_init=0.01, steps=20)
-    assert {r["stage_kernel"] for r in choice["results"]} == {"tiled", "plain", "persistent"}
+    assert {r["stage_kernel"] for r in choice["results"]} == {"tiled", "plain", "staged", "persistent"}
     assert solver.stage_kernel == choice["stage_kernel"]
     outs = []
-    for kernel in ("tiled", "plain", "persistent"):
+    for kernel in ("tiled", "plain", "staged", "persistent"):
         solver.stage_kernel = kernel
         solver.reset()
         solver.start(dt_max=1.0, dt_init=0.01)

@@ -113,7 +113,7 @@ def oracles():
     return out
 
 
-@pytest.mark.parametrize("kernel", ["tiled", "plain", "persistent"])
+@pytest.mark.parametrize("kernel", ["tiled", "plain", "staged", "persistent"])
 @pytest.mark.parametrize("case", list(CASES))
 def test_runs_match_the_oracle_bit_for_bit(case: str, kernel: str, oracles) -> None:
     sc, kinds, values, t_end = channel(case)

@@ -69,7 +69,7 @@ def test_repeat_runs_are_bit_identical(case: str, grid) -> None:
     assert_identical(a, b, run(a, t_end, source_rate=src), run(b, t_end, source_rate=src))
 
 
-@pytest.mark.parametrize("kernel", ["tiled", "plain", "persistent"])
+@pytest.mark.parametrize("kernel", ["tiled", "plain", "staged", "persistent"])
 @pytest.mark.parametrize("fill", [0.5, float("nan")], ids=["wet", "nan"])
 def test_stale_predictor_state_is_never_read(kernel: str, fill: float, grid) -> None:
     h0 = dam(grid)
@@ -80,7 +80,7 @@ def test_stale_predictor_state_is_never_read(kernel: str, fill: float, grid) -> 
     assert_identical(clean, poisoned, run(clean, 30.0), run(poisoned, 30.0))
 
 
-@pytest.mark.parametrize("other", ["plain", "persistent"])
+@pytest.mark.parametrize("other", ["plain", "staged", "persistent"])
 def test_stage_kernels_agree_bit_for_bit(other: str, grid) -> None:
     h0, src, t_end = cases(grid)["wetting"]
     a, b = make(grid, h0, stage_kernel="tiled"), make(grid, h0, stage_kernel=other)
@@ -342,7 +342,7 @@ def test_closed_basin_conserves_volume() -> None:
 
 
 # -- long adaptive run against the FP32 oracle ---------------------------------------------------------------
-@pytest.mark.parametrize("kernel", ["tiled", "plain", "persistent"])
+@pytest.mark.parametrize("kernel", ["tiled", "plain", "staged", "persistent"])
 def test_adaptive_run_with_sources_matches_the_fp32_oracle(kernel: str) -> None:
     g = valley_grid(nx=64, ny=32)
     h0 = sheet(g, nx=64)

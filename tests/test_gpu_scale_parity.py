@@ -12,7 +12,8 @@ oracle's bit for bit, for every stage kernel.
 A fully wet variant (every cell at least 0.5 m deep, 200+ steps) keeps all
 4,096 tiles active: the persistent kernel runs it on its full grid, and on a
 grid of 8 CTAs, where each CTA takes 512 tiles a step, the most its extra-tile
-capacity allows besides its seat.
+capacity allows besides its seat; the staged block kernel runs it on its full
+grid and on 7 CTAs, each restaging its shared memory for about 146 blocks.
 """
 
 from __future__ import annotations
@@ -83,7 +84,7 @@ def assert_same(s, snaps, times, oracle) -> None:
     np.testing.assert_array_equal(s.download_block_flags(), o.download_block_flags())
 
 
-@pytest.mark.parametrize("kernel", ["persistent", "plain", "tiled", "auto"])
+@pytest.mark.parametrize("kernel", ["persistent", "plain", "staged", "tiled", "auto"])
 def test_dam_break_262k_over_2000_steps(scenario, dam_oracle, kernel: str) -> None:
     s, snaps, times = solver_run(scenario, scenario.h0, kernel, 60.0, 20.0)
     assert s.steps_total >= 1000
@@ -93,11 +94,14 @@ def test_dam_break_262k_over_2000_steps(scenario, dam_oracle, kernel: str) -> No
     assert int(flags[:, 1].sum()) > 2 * int((scenario.h0.reshape(-1, 256) > 0).any(axis=1).sum())
 
 
-@pytest.mark.parametrize("kernel, max_grid", [("persistent", None), ("persistent", 8), ("plain", None), ("auto", None)])
+@pytest.mark.parametrize("kernel, max_grid", [("persistent", None), ("persistent", 8), ("plain", None), ("staged", None),
+                                             ("staged", 7), ("auto", None)])
 def test_all_wet_262k_over_200_steps(scenario, wet_oracle, kernel: str, max_grid: int | None) -> None:
     s, snaps, times = solver_run(scenario, wet_start(scenario), kernel, 7.5, 2.5, max_grid)
     assert s.steps_total >= 200
-    if max_grid is not None:
+    if kernel == "persistent" and max_grid is not None:
         assert s.grid(2) == max_grid and 4 * s.n_blocks == 4096 <= max_grid * 513
+    if kernel == "staged" and max_grid is not None:
+        assert s.grid(3) == max_grid  # each CTA stages its blocks one after another
     assert_same(s, snaps, times, wet_oracle)
     assert s.download_block_flags()[:, 1].all()

@@ -112,9 +112,10 @@ def assert_same_bits(a: np.ndarray, b: np.ndarray, what: str) -> None:
     assert bad.size == 0, f"{what}: {bad.size} cells differ from the FP32 oracle (first {bad[:5].tolist()})"
 
 
-@pytest.mark.parametrize("kernel,grid_limit", [("tiled", None), ("plain", None), ("persistent", None), ("tiled", 3),
-                                                ("plain", 5), ("persistent", 3)],
-                         ids=["tiled", "plain", "persistent", "tiled-3ctas", "plain-5ctas", "persistent-3ctas"])
+@pytest.mark.parametrize("kernel,grid_limit", [("tiled", None), ("plain", None), ("staged", None), ("persistent", None),
+                                                ("tiled", 3), ("plain", 5), ("staged", 5), ("persistent", 3)],
+                         ids=["tiled", "plain", "staged", "persistent", "tiled-3ctas", "plain-5ctas", "staged-5ctas",
+                              "persistent-3ctas"])
 @pytest.mark.parametrize("case", list(CASES))
 def test_steps_match_fp64_and_fp32_oracles(case: str, kernel: str, grid_limit, grid) -> None:
     s0 = CASES[case](grid)
