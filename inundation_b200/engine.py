@@ -46,8 +46,8 @@ START, STEP, RETARGET = 0, 1, 2
 STATE_ARRAYS = ("h", "hu", "hv", "h_lo", "h1", "hu1", "hv1", "h1_lo", "clamp_mass")
 KERNELS = {"tiled": 0, "plain": 1, "persistent": 2, "staged": 3}
 # "auto": the persistent kernel while few blocks are active (its phases are latency-bound), the
-# 256-cell block kernel once more than this fraction of blocks is active (issue-bound work), unless
-# every active tile still has a CTA of the persistent grid to itself (a small mesh).
+# staged 256-cell block kernel once more than this fraction of blocks is active (work for the
+# whole GPU), unless every active tile still has a CTA of the persistent grid to itself (a small mesh).
 AUTO_DENSE_FRACTION = 0.25
 PERSISTENT_EXTRA_TILES = 512  # kExtraCap of the persistent kernel
 
@@ -87,7 +87,7 @@ class ResidentEngine:
     # "plain" (256-cell blocks, direct loads), "staged" (256-cell blocks staged by bulk copies),
     # "persistent" (the tiled stages and the rest of the
     # step in one cooperative launch per submit, phases separated by grid barriers) or "auto"
-    # (persistent or plain by the active fraction read after every submit). All give the same bits.
+    # (persistent or staged by the active fraction read after every submit). All give the same bits.
     stage_kernel: str = "auto"
 
     def _init_engine(
@@ -181,7 +181,7 @@ class ResidentEngine:
         if self.stage_kernel == "auto":
             dense = self._active_blocks > AUTO_DENSE_FRACTION * self.n_blocks
             seated = 4 * self._active_blocks <= self.grid(KERNELS["persistent"])
-            return KERNELS["persistent"] if self._persistent_fits and (seated or not dense) else KERNELS["plain"]
+            return KERNELS["persistent"] if self._persistent_fits and (seated or not dense) else KERNELS["staged"]
         if self.stage_kernel not in KERNELS:
             raise ValueError(f"stage_kernel must be one of {sorted(KERNELS)} or 'auto', got {self.stage_kernel!r}")
         return KERNELS[self.stage_kernel]

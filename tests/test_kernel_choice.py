@@ -2,7 +2,7 @@
 
 The rule: the persistent whole-step kernel while at most a quarter of the blocks
 are active, or while every active 64-cell tile has a CTA of its grid to itself
-(a small mesh); the 256-cell block kernel otherwise, and always when the
+(a small mesh); the staged 256-cell block kernel otherwise, and always when the
 persistent grid cannot hold a step (one seat and 512 other tiles per CTA).
 Also the two-sum guard's verdict on a probe's words.
 """
@@ -13,7 +13,7 @@ import pytest
 
 from inundation_b200.engine import KERNELS, PERSISTENT_EXTRA_TILES, ResidentEngine
 
-PERSISTENT, PLAIN = KERNELS["persistent"], KERNELS["plain"]
+PERSISTENT, STAGED = KERNELS["persistent"], KERNELS["staged"]
 
 
 def engine(n_blocks: int, active: int, sms: int = 148, per_sm: int = 4, max_grid: int | None = None):
@@ -33,11 +33,11 @@ def engine(n_blocks: int, active: int, sms: int = 148, per_sm: int = 4, max_grid
     [
         (3907, 140, PERSISTENT),  # 1M-cell dam break: 3.6 % of the blocks
         (3907, 976, PERSISTENT),  # a quarter active (976.75), no more
-        (3907, 977, PLAIN),  # past a quarter: issue-bound work for the block kernel
-        (3907, 3907, PLAIN),  # all wet
+        (3907, 977, STAGED),  # past a quarter: issue-bound work for the block kernel
+        (3907, 3907, STAGED),  # all wet
         (32, 32, PERSISTENT),  # 8k-cell lake at rest: 128 tiles, one CTA each
         (148, 148, PERSISTENT),  # 592 tiles on 592 CTAs
-        (149, 149, PLAIN),  # one tile more than CTAs, all active
+        (149, 149, STAGED),  # one tile more than CTAs, all active
     ],
 )
 def test_auto_rule(n_blocks: int, active: int, want: int) -> None:
@@ -51,9 +51,9 @@ def test_persistent_needs_room_for_every_tile() -> None:
     assert engine(fits, 1)._kernel == PERSISTENT
     too_many = fits + 1
     assert not engine(too_many, 1)._persistent_fits
-    assert engine(too_many, 1)._kernel == PLAIN  # sparse, but a step could not find every tile a CTA
+    assert engine(too_many, 1)._kernel == STAGED  # sparse, but a step could not find every tile a CTA
     # a capped grid shrinks both the capacity and the "one CTA per tile" case
-    assert engine(32, 32, max_grid=64)._kernel == PLAIN
+    assert engine(32, 32, max_grid=64)._kernel == STAGED
 
 
 def test_explicit_choice_and_unknown_names() -> None:
