@@ -167,6 +167,12 @@ __global__ void __launch_bounds__(kThreads, SWE_BLOCK_MIN_CTAS)
 #ifndef SWE_STAGED_MIN_CTAS
 #define SWE_STAGED_MIN_CTAS 5
 #endif
+// 1: the corrector also stages the committed state (10 columns); 0: it reads it from global memory
+// at the update (6 columns, less shared memory per CTA).
+#ifndef SWE_STAGED_COMMITTED
+#define SWE_STAGED_COMMITTED 1
+#endif
+__host__ __device__ constexpr uint32_t staged_cols(int stage) { return (stage && SWE_STAGED_COMMITTED) ? 10u : 6u; }
 
 struct StagedPlan {
     uint32_t capE, capS, nc, total;
@@ -204,7 +210,7 @@ __global__ void __launch_bounds__(kThreads, SWE_STAGED_MIN_CTAS)
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint32_t red[kThreads / 32];
     __shared__ uint32_t fields[2][8];
-    constexpr uint32_t nc = STAGE ? 10u : 6u;
+    constexpr uint32_t nc = staged_cols(STAGE);
     const StagedPlan L = staged_plan(m.max_tile_edges, m.max_blk_slots, nc);
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem);
     int32_t *Rcl = reinterpret_cast<int32_t *>(smem + 128);
@@ -341,6 +347,19 @@ __global__ void __launch_bounds__(kThreads, SWE_STAGED_MIN_CTAS)
         bool wet = false;
         uint32_t bound = kNoBound;
         if (tid < cells) {
+            const uint32_t i = b * kBlockCells + tid;
+            float h0 = 0.0f, hu0 = 0.0f, hv0 = 0.0f, lo0 = 0.0f;  // the corrector's committed state
+            if (STAGE && nc == 10u) {
+                h0 = C[6 * kBlockCells + tid];
+                hu0 = C[7 * kBlockCells + tid];
+                hv0 = C[8 * kBlockCells + tid];
+                lo0 = C[9 * kBlockCells + tid];
+            } else if (STAGE) {  // in flight during the gather
+                h0 = s.h[i];
+                hu0 = s.hu[i];
+                hv0 = s.hv[i];
+                lo0 = s.h_lo[i];
+            }
             float sdh = 0.0f, sdhu = 0.0f, sdhv = 0.0f, lam = 0.0f;
             const uint32_t q0 = Cp[tid] - Cp[0], q1 = Cp[tid + 1] - Cp[0];
             for (uint32_t q = q0; q < q1; ++q) {
@@ -358,20 +377,16 @@ __global__ void __launch_bounds__(kThreads, SWE_STAGED_MIN_CTAS)
                 }
                 if (STAGE == 1) lam += __int_as_float(W5[j]);
             }
-            const uint32_t i = b * kBlockCells + tid;
             if (sums) {
                 const uint32_t n = m.n_blocks * kBlockCells;
                 sums[i] = sdh;
                 sums[n + i] = sdhu;
                 sums[2 * n + i] = sdhv;
             }
-            const float *cc = C + 6 * kBlockCells;
             update_cell<STAGE, COMP, CLAMP>(s, p, cfl, dt, i, C[4 * kBlockCells + tid], C[5 * kBlockCells + tid],
                                             C[tid], C[kBlockCells + tid], C[2 * kBlockCells + tid],
-                                            C[3 * kBlockCells + tid], STAGE ? cc[tid] : 0.0f,
-                                            STAGE ? cc[kBlockCells + tid] : 0.0f,
-                                            STAGE ? cc[2 * kBlockCells + tid] : 0.0f,
-                                            STAGE ? cc[3 * kBlockCells + tid] : 0.0f, sdh, sdhu, sdhv, lam, wet, bound);
+                                            C[3 * kBlockCells + tid], h0, hu0, hv0, lo0, sdh, sdhu, sdhv, lam, wet,
+                                            bound);
         }
         if (STAGE == 1) {
             const int any_wet = __syncthreads_or(wet);
@@ -420,7 +435,7 @@ int launch_stage(const swe_mesh_t *m, const swe_state_t *s, const swe_params_t *
     if (p->kernel == 3u) {
         if (!m->blk_lcsr || !m->blk_lcsr_ptr) return SWE_ERR_ARGUMENT;
         auto kern = stage_staged_kernel<STAGE, COMP, CLAMP, OPEN>;
-        const size_t bytes = staged_plan(m->max_tile_edges, m->max_blk_slots, STAGE ? 10u : 6u).total;
+        const size_t bytes = staged_plan(m->max_tile_edges, m->max_blk_slots, staged_cols(STAGE)).total;
         int rc = set_smem(kern, bytes);
         if (rc) return rc;
         const uint32_t grid = (p->grid == 0u || p->grid > m->n_blocks) ? m->n_blocks : p->grid;
@@ -464,7 +479,7 @@ template <int STAGE, bool COMP, bool CLAMP>
 int configure_stage(const swe_mesh_t *m) {
     const size_t block = block_smem_bytes(m->max_tile_edges);
     const size_t tiled = tile_plan(m->max_sub_edges, m->max_sub_slots, STAGE ? 10u : 6u).total;
-    const size_t staged = staged_plan(m->max_tile_edges, m->max_blk_slots, STAGE ? 10u : 6u).total;
+    const size_t staged = staged_plan(m->max_tile_edges, m->max_blk_slots, staged_cols(STAGE)).total;
     int rc = set_smem(stage_block_kernel<STAGE, COMP, CLAMP, false>, block);
     if (!rc) rc = set_smem(stage_block_kernel<STAGE, COMP, CLAMP, true>, block);
     if (!rc) rc = set_smem(stage_staged_kernel<STAGE, COMP, CLAMP, false>, staged);
@@ -503,7 +518,7 @@ int swe_configure(const swe_mesh_t *mesh, int kernel, int *blocks_per_sm) {
     } else if (kernel == 3) {
         err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
             blocks_per_sm, stage_staged_kernel<1, true, false, false>, kThreads,
-            staged_plan(mesh->max_tile_edges, mesh->max_blk_slots, 10u).total);
+            staged_plan(mesh->max_tile_edges, mesh->max_blk_slots, staged_cols(1)).total);
     } else {
         err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, stage_block_kernel<1, true, false, false>, kThreads,
                                                             block_smem_bytes(mesh->max_tile_edges));
