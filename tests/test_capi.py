@@ -66,6 +66,22 @@ def test_status_strings_and_argument_checks(lib: ctypes.CDLL) -> None:
     assert lib.swe_configure(None, 0, None) == 1
 
 
+def test_stage_refuses_kernel_2_and_a_staged_kernel_without_its_csr(lib: ctypes.CDLL) -> None:
+    """swe_stage runs kernels 0, 1 and 3; kernel 3 also needs the regrouped block CSR.
+
+    Placeholder addresses again: both refusals come from host-side checks before any device call.
+    """
+    mesh = native.SweMesh(n_cells=256, n_blocks=1, max_tile_edges=64, n_inst=1, max_sub_edges=64, max_sub_slots=64)
+    for name, kind in native.SweMesh._fields_:
+        if kind is native._P and name not in ("open_cond", "blk_lcsr", "blk_lcsr_ptr"):
+            setattr(mesh, name, 0x10000)
+    state = native.SweState(**{name: 0x20000 for name, _ in native.SweState._fields_})
+    for kernel in (2, 3, 4):
+        params = native.SweParams(g=9.81, dry_tol=1e-4, cfl=0.8, compensated=1, active_set=1, kernel=kernel)
+        for stage in (0, 1):
+            assert lib.swe_stage(ctypes.byref(mesh), ctypes.byref(state), ctypes.byref(params), stage, None) == 1
+
+
 def test_whole_steps_refuse_a_misaligned_dt_buffer(lib: ctypes.CDLL) -> None:
     """Kernel 2 publishes each dt as a 64-bit pair in dt words 2..3: dt_buf must be 16-byte aligned.
 
