@@ -234,10 +234,11 @@ __device__ __forceinline__ void tally_open(float *vol, uint32_t k, float v) {
 
 // -- host helpers --------------------------------------------------------------------------------
 inline int check_launch() { return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ERR_CUDA; }
+constexpr size_t kMaxSmem = 227 * 1024;  // dynamic shared memory a CTA may opt in to
 
 template <typename K>
 inline int set_smem(K kernel, size_t bytes) {
-    if (bytes > 227 * 1024) return SWE_ERR_TOO_LARGE;
+    if (bytes > kMaxSmem) return SWE_ERR_TOO_LARGE;
     if (bytes > 48 * 1024 &&
         cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)) != cudaSuccess)
         return SWE_ERR_CUDA;

@@ -482,8 +482,9 @@ int configure_stage(const swe_mesh_t *m) {
     const size_t staged = staged_plan(m->max_tile_edges, m->max_blk_slots, staged_cols(STAGE)).total;
     int rc = set_smem(stage_block_kernel<STAGE, COMP, CLAMP, false>, block);
     if (!rc) rc = set_smem(stage_block_kernel<STAGE, COMP, CLAMP, true>, block);
-    if (!rc) rc = set_smem(stage_staged_kernel<STAGE, COMP, CLAMP, false>, staged);
-    if (!rc) rc = set_smem(stage_staged_kernel<STAGE, COMP, CLAMP, true>, staged);
+    // a mesh whose largest block does not fit the staged kernel's shared memory runs the others
+    if (!rc && staged <= kMaxSmem) rc = set_smem(stage_staged_kernel<STAGE, COMP, CLAMP, false>, staged);
+    if (!rc && staged <= kMaxSmem) rc = set_smem(stage_staged_kernel<STAGE, COMP, CLAMP, true>, staged);
     if (!rc) rc = set_smem(stage_tiled_kernel<STAGE, COMP, CLAMP, false>, tiled);
     if (!rc) rc = set_smem(stage_tiled_kernel<STAGE, COMP, CLAMP, true>, tiled);
     return rc;
@@ -516,9 +517,11 @@ int swe_configure(const swe_mesh_t *mesh, int kernel, int *blocks_per_sm) {
             blocks_per_sm, stage_tiled_kernel<1, true, false, false>, kTileThreads,
             tile_plan(mesh->max_sub_edges, mesh->max_sub_slots, 10u).total);
     } else if (kernel == 3) {
-        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            blocks_per_sm, stage_staged_kernel<1, true, false, false>, kThreads,
-            staged_plan(mesh->max_tile_edges, mesh->max_blk_slots, staged_cols(1)).total);
+        const size_t bytes = staged_plan(mesh->max_tile_edges, mesh->max_blk_slots, staged_cols(1)).total;
+        *blocks_per_sm = 0;  // 0: this mesh's blocks do not fit
+        err = bytes > kMaxSmem ? cudaSuccess
+                               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                                     blocks_per_sm, stage_staged_kernel<1, true, false, false>, kThreads, bytes);
     } else {
         err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, stage_block_kernel<1, true, false, false>, kThreads,
                                                             block_smem_bytes(mesh->max_tile_edges));

@@ -163,6 +163,8 @@ class ResidentEngine:
             with torch.cuda.device(self.device):
                 native.check(self._lib.swe_configure(ctypes.byref(m), kernel, ctypes.byref(per_sm)), "swe_configure")
             self._per_sm[kernel] = max(1, per_sm.value)
+            if kernel == KERNELS["staged"]:  # 0: the mesh's largest block does not fit its shared memory
+                self._staged_fits = per_sm.value > 0
         self.ctas_per_sm: int | None = None  # None: as many as fit
         self.max_grid: int | None = None  # an upper bound on the persistent CTAs (None: none)
 
@@ -181,7 +183,9 @@ class ResidentEngine:
         if self.stage_kernel == "auto":
             dense = self._active_blocks > AUTO_DENSE_FRACTION * self.n_blocks
             seated = 4 * self._active_blocks <= self.grid(KERNELS["persistent"])
-            return KERNELS["persistent"] if self._persistent_fits and (seated or not dense) else KERNELS["staged"]
+            if self._persistent_fits and (seated or not dense):
+                return KERNELS["persistent"]
+            return KERNELS["staged"] if self._staged_fits else KERNELS["plain"]
         if self.stage_kernel not in KERNELS:
             raise ValueError(f"stage_kernel must be one of {sorted(KERNELS)} or 'auto', got {self.stage_kernel!r}")
         return KERNELS[self.stage_kernel]

@@ -25,6 +25,7 @@ def engine(n_blocks: int, active: int, sms: int = 148, per_sm: int = 4, max_grid
     e._per_sm = {k: per_sm for k in KERNELS.values()}
     e.ctas_per_sm = None
     e.max_grid = max_grid
+    e._staged_fits = True
     return e
 
 
@@ -54,6 +55,13 @@ def test_persistent_needs_room_for_every_tile() -> None:
     assert engine(too_many, 1)._kernel == STAGED  # sparse, but a step could not find every tile a CTA
     # a capped grid shrinks both the capacity and the "one CTA per tile" case
     assert engine(32, 32, max_grid=64)._kernel == STAGED
+
+
+def test_blocks_too_large_for_the_staged_kernel_run_the_plain_one() -> None:
+    e = engine(3907, 3907)
+    e._staged_fits = False
+    assert e._kernel == KERNELS["plain"]
+    assert engine(3907, 140)._kernel == PERSISTENT
 
 
 def test_explicit_choice_and_unknown_names() -> None:
