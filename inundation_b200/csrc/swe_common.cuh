@@ -71,6 +71,27 @@ __device__ __forceinline__ void load_state(const swe_state_t &s, int c, float &h
     }
 }
 
+// A corrector tile's two verdicts after one CTA barrier: whether any thread's cell is wet and the
+// minimum of the threads' CFL bounds, both valid in warp 0 (scratch: 2 words per warp). Every thread
+// has finished its update when the barrier passes; the scratch is next written after a later barrier.
+__device__ __forceinline__ void tile_verdicts(bool wet, uint32_t bound, uint32_t *scratch, bool &any_wet,
+                                              uint32_t &bmin) {
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u, nw = blockDim.x >> 5;
+    const uint32_t m = __reduce_min_sync(0xFFFFFFFFu, bound);
+    const bool w = __any_sync(0xFFFFFFFFu, wet);
+    if (lane == 0) {
+        scratch[warp] = m;
+        scratch[nw + warp] = w ? 1u : 0u;
+    }
+    __syncthreads();
+    any_wet = false;
+    bmin = kNoBound;
+    if (warp == 0) {
+        bmin = __reduce_min_sync(0xFFFFFFFFu, lane < nw ? scratch[lane] : kNoBound);
+        any_wet = __any_sync(0xFFFFFFFFu, lane < nw && scratch[nw + lane] != 0u);
+    }
+}
+
 __device__ __forceinline__ uint32_t block_min_any(uint32_t v, uint32_t *scratch) {
     v = __reduce_min_sync(0xFFFFFFFFu, v);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;

@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(kThreads, SWE_BLOCK_MIN_CTAS)
     stage_block_kernel(swe_mesh_t m, swe_state_t s, Phys p, float cfl, float *sums) {
     const uint32_t cap = (m.max_tile_edges + 3u) & ~3u;
     const TileSmem t = tile_smem(cap);
-    __shared__ uint32_t red[kThreads / 32];
+    __shared__ uint32_t red[2 * kThreads / 32];
     const uint32_t count = s.sched[kSchedActive];
     uint64_t computed = 0;
 
@@ -139,8 +139,9 @@ __global__ void __launch_bounds__(kThreads, SWE_BLOCK_MIN_CTAS)
                                             lo0, sdh, sdhu, sdhv, lam, wet, bound);
         }
         if (STAGE == 1) {
-            const int any_wet = __syncthreads_or(wet);
-            const uint32_t bmin = block_min_any(bound, red);
+            bool any_wet;
+            uint32_t bmin;
+            tile_verdicts(wet, bound, red, any_wet, bmin);
             if (threadIdx.x == 0) {
                 s.blk[kBlkWords * b + kBlkWet] = any_wet ? 1u : 0u;
                 if (bmin != kNoBound) atomicMin(&s.dt_buf[kDtWords * inst + 1], bmin);
@@ -208,7 +209,7 @@ template <int STAGE, bool COMP, bool CLAMP, bool OPEN>
 __global__ void __launch_bounds__(kThreads, SWE_STAGED_MIN_CTAS)
     stage_staged_kernel(swe_mesh_t m, swe_state_t s, Phys p, float cfl, float *sums) {
     extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ uint32_t red[kThreads / 32];
+    __shared__ uint32_t red[2 * kThreads / 32];
     __shared__ uint32_t fields[2][8];
     constexpr uint32_t nc = staged_cols(STAGE);
     const StagedPlan L = staged_plan(m.max_tile_edges, m.max_blk_slots, nc);
@@ -389,8 +390,9 @@ __global__ void __launch_bounds__(kThreads, SWE_STAGED_MIN_CTAS)
                                             bound);
         }
         if (STAGE == 1) {
-            const int any_wet = __syncthreads_or(wet);
-            const uint32_t bmin = block_min_any(bound, red);
+            bool any_wet;
+            uint32_t bmin;
+            tile_verdicts(wet, bound, red, any_wet, bmin);
             if (tid == 0) {
                 s.blk[kBlkWords * b + kBlkWet] = any_wet ? 1u : 0u;
                 if (bmin != kNoBound) atomicMin(&s.dt_buf[kDtWords * m.block_inst[b] + 1], bmin);

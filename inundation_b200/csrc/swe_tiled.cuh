@@ -307,7 +307,7 @@ __device__ __forceinline__ void tile_issue(const swe_mesh_t &m, const swe_state_
 template <int TPB>
 struct TiledShared {
     uint32_t late[3];  // LateDt's slots
-    uint32_t red[TPB / 32];
+    uint32_t red[2 * TPB / 32];
     uint4 items[2];
     uint32_t dts[2];
     uint32_t count;
@@ -341,7 +341,7 @@ __host__ __device__ inline size_t tiled_smem_bytes(uint32_t max_edges, uint32_t 
 // corrector in com_col..com_col+3. F == nullptr: the flux words overwrite the
 // consumed records; otherwise they go to F (7 x capE words) and the records stay.
 // keep_pred: the new state also goes to columns 6..9 (predictor) or 0..3
-// (corrector). Returns, in the corrector, whether a cell of the tile is wet.
+// (corrector). Returns, in the corrector and to warp 0, whether a cell of the tile is wet.
 // OPEN: the mesh has open edges (right cell -2 - k), with ghosts and tallies.
 template <int STAGE, bool COMP, bool CLAMP, int TPB, bool OPEN>
 __device__ __forceinline__ bool tile_compute(const swe_mesh_t &m, const swe_state_t &s, const Phys &p, float cfl,
@@ -463,14 +463,15 @@ __device__ __forceinline__ bool tile_compute(const swe_mesh_t &m, const swe_stat
                                         keep_pred ? B.c + (STAGE ? 0 : 6) * kTileCells + tid : nullptr);
     }
     if (STAGE == 1) {
-        const int any_wet = __syncthreads_or(wet);
-        const uint32_t bmin = block_min_any(bound, red);
+        bool any_wet;
+        uint32_t bmin;
+        tile_verdicts(wet, bound, red, any_wet, bmin);
         if (tid == 0) {
             if (any_wet) s.blk[kBlkWords * b + kBlkWet] = 1u;
             if (bmin != kNoBound) atomicMin(&s.dt_buf[kDtWords * it.inst + 1], bmin);
             computed += it.cells;
         }
-        return any_wet != 0;
+        return any_wet;  // valid in warp 0
     }
     return false;
 }
