@@ -28,7 +28,8 @@ namespace swe {
 // after sources). Tiles without a seat wait in a queue: at the start of a
 // launch every active tile (the block list), later the tiles of blocks that
 // become active (pushed by the step that first marks them) and the tiles a
-// CTA computed besides its seat (pushed back every step). CTAs without a seat
+// CTA computed besides its seat (pushed back every step, except the first of
+// them, which the CTA keeps and stages while its seat computes). CTAs without a seat
 // take queued tiles first and seat the first one; a CTA with a seat takes more
 // only after computing its seat, and streams those through its second buffer.
 // A sparse step's critical path is then a few dependent global accesses (the
@@ -73,6 +74,8 @@ struct SeatShared {
     uint32_t take;            // a taken tile (kNoTile: the queue is empty)
     uint4 take_item;
     uint32_t take_dt;
+    uint32_t kept;            // the other tile this CTA computed last step, kept for this one (kNoTile: none)
+    uint4 kept_item;
 };
 
 __device__ __forceinline__ uint4 tile_item(const swe_mesh_t &m, uint32_t t, uint32_t inst) {
@@ -214,6 +217,8 @@ __device__ bool seat_predictor(const swe_mesh_t &m, const swe_state_t &s, const 
     float *F = reinterpret_cast<float *>(smem + L.total);
     const TileBuf B0 = tile_buf(smem, L, 0u), B1 = tile_buf(smem, L, 1u);
     const uint32_t tid = threadIdx.x;
+    const uint32_t kept = ss.kept;
+    bool kept_issued = false;
     if (!OPEN && step > 0u && ss.seat != kNoTile) {
         // The seat's predictor starts before its activity and dt are known: both arrive
         // while its fluxes are computed (the update of an inactive seat keeps nothing
@@ -227,6 +232,9 @@ __device__ bool seat_predictor(const swe_mesh_t &m, const swe_state_t &s, const 
         // the queue's length (final since the last barrier) arrives with them
         const LateDt late{dt_pair(s, it.inst), s.marks + 2u * b, s.sched + kSchedQProd + (step & 1u), epoch,
                           all_active ? 1u : 0u, sh.late};
+        // the kept tile's records and state are staged while the seat computes
+        kept_issued = kept != kNoTile;
+        if (kept_issued && tid < 32u) seat_issue<0>(m, s, ss.kept_item, B1, false);
         tile_compute<0, COMP, CLAMP, kPersistThreads, OPEN>(m, s, p, cfl, B0, it, 0.0f, 0u, 6u, F, L.capE, sh.red,
                                                             computed, true, nullptr, &late);
         fence_proxy_async();
@@ -289,6 +297,39 @@ __device__ bool seat_predictor(const swe_mesh_t &m, const swe_state_t &s, const 
             const uint32_t bits = __ballot_sync(0xFFFFFFFFu, act);
             if (lane == 0) ss.ring_active[w] = bits;
         }
+    }
+    // The kept tile first (it is in no queue): computed when it is still active this step,
+    // dropped otherwise, with the block flag handled as for a tile taken from the queue.
+    if (kept != kNoTile) {
+        if (!kept_issued && tid < 32u) seat_issue<0>(m, s, ss.kept_item, B1, false);
+        if (tid == 0) {
+            const Item ki = unpack(ss.kept_item);
+            const uint32_t b = ki.tile >> 2;
+            const uint32_t dt = step_dt(s, ki.inst, step, epoch);
+            const bool active = all_active || s.marks[2u * b] == epoch;
+            const uint32_t flag = s.blk[kBlkWords * b + kBlkActive];
+            bool use = false;
+            if (dt != 0u) {  // a no-op step keeps the block's flags
+                if ((ki.tile & 3u) == 0u && flag != (active ? 1u : 0u)) s.blk[kBlkWords * b + kBlkActive] = active;
+                use = active;
+            }
+            ss.take = use ? ki.tile : kNoTile;
+            ss.take_dt = dt;
+            ss.kept = kNoTile;
+            if (use) {
+                ss.extra[ss.n_extra] = ss.kept_item;
+                ss.extra_dt[ss.n_extra] = dt;
+                ss.n_extra += 1u;
+            }
+        }
+        if (!seat_wait(s, B1, ph, 1u)) return false;
+        if (ss.take != kNoTile) {
+            tile_compute<0, COMP, CLAMP, kPersistThreads, OPEN>(m, s, p, cfl, B1, unpack(ss.kept_item),
+                                                                __uint_as_float(ss.take_dt), 0u, 6u, F, L.capE,
+                                                                sh.red, computed, false);
+            fence_proxy_async();
+        }
+        __syncthreads();
     }
     for (;;) {
         if (ss.seat != kNoTile && ss.n_extra >= kExtraCap) break;
@@ -380,11 +421,17 @@ __device__ bool seat_corrector(const swe_mesh_t &m, const swe_state_t &s, const 
         fence_proxy_async();
         __syncthreads();
     }
-    if (n) {  // the other tiles wait in the next step's queue again (checked for activity when taken)
+    // The first other tile stays with this CTA for the next step (checked for activity
+    // then); the rest wait in the next step's queue again (checked when taken).
+    if (n && tid == 0) {
+        ss.kept = unpack(ss.extra[0]).tile;
+        ss.kept_item = ss.extra[0];
+    }
+    if (n > 1u) {
         uint32_t *q = tile_queue(m, s, qpar);
-        if (tid == 0) ss.qlen = atomicAdd(&s.sched[kSchedQProd + qpar], n);
+        if (tid == 0) ss.qlen = atomicAdd(&s.sched[kSchedQProd + qpar], n - 1u);
         __syncthreads();
-        for (uint32_t w = tid; w < n; w += blockDim.x) q[ss.qlen + w] = unpack(ss.extra[w]).tile;
+        for (uint32_t w = tid; w + 1u < n; w += blockDim.x) q[ss.qlen + w] = unpack(ss.extra[w + 1u]).tile;
     }
     return true;
 }
@@ -446,7 +493,7 @@ __global__ void __launch_bounds__(kPersistThreads, 1024 / kPersistThreads)
         mbar_init(reinterpret_cast<uint64_t *>(smem) + 1, 1u);
         fence_barrier_init();
         epoch0 = *reinterpret_cast<volatile uint32_t *>(s.sched + kSchedEpoch);  // before any CTA's first barrier
-        ss.seat = ss.staged = kNoTile;
+        ss.seat = ss.staged = ss.kept = kNoTile;
         ss.state_ok = 0u;
         if (blockIdx.x == 0) {  // the queues of this launch start empty (first used after the first barrier)
             for (int k = 0; k < 2; ++k) {
