@@ -168,12 +168,8 @@ __global__ void __launch_bounds__(kThreads, SWE_BLOCK_MIN_CTAS)
 #ifndef SWE_STAGED_MIN_CTAS
 #define SWE_STAGED_MIN_CTAS 5
 #endif
-// 1: the corrector also stages the committed state (10 columns); 0: it reads it from global memory
-// at the update (6 columns, less shared memory per CTA).
-#ifndef SWE_STAGED_COMMITTED
-#define SWE_STAGED_COMMITTED 1
-#endif
-__host__ __device__ constexpr uint32_t staged_cols(int stage) { return (stage && SWE_STAGED_COMMITTED) ? 10u : 6u; }
+// Cell columns a stage stages: the input state, area and n, and in the corrector the committed state.
+__host__ __device__ constexpr uint32_t staged_cols(int stage) { return stage ? 10u : 6u; }
 
 struct StagedPlan {
     uint32_t capE, capS, nc, total;
@@ -350,16 +346,11 @@ __global__ void __launch_bounds__(kThreads, SWE_STAGED_MIN_CTAS)
         if (tid < cells) {
             const uint32_t i = b * kBlockCells + tid;
             float h0 = 0.0f, hu0 = 0.0f, hv0 = 0.0f, lo0 = 0.0f;  // the corrector's committed state
-            if (STAGE && nc == 10u) {
+            if (STAGE) {
                 h0 = C[6 * kBlockCells + tid];
                 hu0 = C[7 * kBlockCells + tid];
                 hv0 = C[8 * kBlockCells + tid];
                 lo0 = C[9 * kBlockCells + tid];
-            } else if (STAGE) {  // in flight during the gather
-                h0 = s.h[i];
-                hu0 = s.hu[i];
-                hv0 = s.hv[i];
-                lo0 = s.h_lo[i];
             }
             float sdh = 0.0f, sdhu = 0.0f, sdhv = 0.0f, lam = 0.0f;
             const uint32_t q0 = Cp[tid] - Cp[0], q1 = Cp[tid + 1] - Cp[0];
