@@ -76,6 +76,12 @@ struct SeatShared {
     uint32_t take_dt;
     uint32_t kept;            // the other tile this CTA computed last step, kept for this one (kNoTile: none)
     uint4 kept_item;
+    uint32_t kept_ring_block; // the block whose two-ring kept_ring holds (kNoTile: none)
+    uint32_t kept_ring_n;
+    uint32_t kept_forced;
+    uint32_t kept_bits_step;  // step + 1 of the step kept_ring_active describes (0: none)
+    uint32_t kept_ring[kRingCache];
+    uint32_t kept_ring_active[kRingCache / 32];
 };
 
 __device__ __forceinline__ uint4 tile_item(const swe_mesh_t &m, uint32_t t, uint32_t inst) {
@@ -322,6 +328,33 @@ __device__ bool seat_predictor(const swe_mesh_t &m, const swe_state_t &s, const 
                 ss.n_extra += 1u;
             }
         }
+        if (!OPEN && !all_active && tid >= 64u && tid < 96u) {
+            // warp 2: the kept tile's block two-ring (read once while the tile stays kept) and
+            // which of its blocks are active now, for its corrector's marks as the seat has them
+            const uint32_t lane = tid & 31u, b = unpack(ss.kept_item).tile >> 2;
+            if (ss.kept_ring_block != b) {
+                const uint32_t k0 = m.ring_ptr[b], rn = m.ring_ptr[b + 1] - k0;
+                if (rn <= kRingCache)
+                    for (uint32_t r = lane; r < rn; r += 32u) ss.kept_ring[r] = m.ring_idx[k0 + r];
+                if (lane == 0) {
+                    ss.kept_ring_n = rn;
+                    ss.kept_forced = s.blk[kBlkWords * b + kBlkForced];
+                }
+                __syncwarp();
+                if (lane == 0) ss.kept_ring_block = b;
+            }
+            __syncwarp();
+            const uint32_t rn = ss.kept_ring_n;
+            if (rn <= kRingCache) {
+                for (uint32_t w = 0; w * 32u < rn; ++w) {
+                    const uint32_t k = w * 32u + lane;
+                    const bool act = k < rn && s.marks[2u * ss.kept_ring[k]] == epoch;
+                    const uint32_t bits = __ballot_sync(0xFFFFFFFFu, act);
+                    if (lane == 0) ss.kept_ring_active[w] = bits;
+                }
+                if (lane == 0) ss.kept_bits_step = step + 1u;
+            }
+        }
         if (!seat_wait(s, B1, ph, 1u)) return false;
         if (ss.take != kNoTile) {
             tile_compute<0, COMP, CLAMP, kPersistThreads, OPEN>(m, s, p, cfl, B1, unpack(ss.kept_item),
@@ -416,8 +449,12 @@ __device__ bool seat_corrector(const swe_mesh_t &m, const swe_state_t &s, const 
         const Item it = unpack(ss.extra[w]);
         const bool wet = tile_compute<1, COMP, CLAMP, kPersistThreads, OPEN>(
             m, s, p, cfl, B1, it, __uint_as_float(ss.extra_dt[w]), 0u, 6u, F, L.capE, sh.red, computed, false);
-        if (!all_active && tid < 32u && (wet || s.blk[kBlkWords * (it.tile >> 2) + kBlkForced] != 0u))
-            mark_ring(m, s, it.tile >> 2, epoch, next, qpar, nullptr, 0u);
+        // the kept tile's block has its two-ring and this step's active bits cached
+        const uint32_t eb = it.tile >> 2;
+        const bool cached = ss.kept_ring_block == eb && ss.kept_bits_step == step + 1u && ss.kept_ring_n <= kRingCache;
+        if (!all_active && tid < 32u && (wet || (cached ? ss.kept_forced : s.blk[kBlkWords * eb + kBlkForced]) != 0u))
+            mark_ring(m, s, eb, epoch, next, qpar, cached ? ss.kept_ring : nullptr, ss.kept_ring_n,
+                      cached ? ss.kept_ring_active : nullptr);
         fence_proxy_async();
         __syncthreads();
     }
@@ -493,7 +530,8 @@ __global__ void __launch_bounds__(kPersistThreads, 1024 / kPersistThreads)
         mbar_init(reinterpret_cast<uint64_t *>(smem) + 1, 1u);
         fence_barrier_init();
         epoch0 = *reinterpret_cast<volatile uint32_t *>(s.sched + kSchedEpoch);  // before any CTA's first barrier
-        ss.seat = ss.staged = ss.kept = kNoTile;
+        ss.seat = ss.staged = ss.kept = ss.kept_ring_block = kNoTile;
+        ss.kept_bits_step = 0u;
         ss.state_ok = 0u;
         if (blockIdx.x == 0) {  // the queues of this launch start empty (first used after the first barrier)
             for (int k = 0; k < 2; ++k) {
