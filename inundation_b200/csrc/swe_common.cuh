@@ -71,11 +71,11 @@ __device__ __forceinline__ void load_state(const swe_state_t &s, int c, float &h
     }
 }
 
-// A corrector tile's two verdicts after one CTA barrier: whether any thread's cell is wet and the
+// A corrector tile's two results after one CTA barrier: whether any thread's cell is wet and the
 // minimum of the threads' CFL bounds, both valid in warp 0 (scratch: 2 words per warp). Every thread
 // has finished its update when the barrier passes; the scratch is next written after a later barrier.
-__device__ __forceinline__ void tile_verdicts(bool wet, uint32_t bound, uint32_t *scratch, bool &any_wet,
-                                              uint32_t &bmin) {
+__device__ __forceinline__ void tile_outcome(bool wet, uint32_t bound, uint32_t *scratch, bool &any_wet,
+                                             uint32_t &bmin) {
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u, nw = blockDim.x >> 5;
     const uint32_t m = __reduce_min_sync(0xFFFFFFFFu, bound);
     const bool w = __any_sync(0xFFFFFFFFu, wet);
@@ -108,7 +108,7 @@ __device__ __forceinline__ uint32_t block_min_any(uint32_t v, uint32_t *scratch)
     return r;
 }
 
-// -- bulk copies (TMA, 1-D, no multicast) into shared memory on an mbarrier --------------------
+// -- bulk copies (TMA, 1-D, into this CTA's own shared memory) on an mbarrier --------------------
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }

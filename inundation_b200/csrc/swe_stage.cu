@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(kThreads, SWE_BLOCK_MIN_CTAS)
         if (STAGE == 1) {
             bool any_wet;
             uint32_t bmin;
-            tile_verdicts(wet, bound, red, any_wet, bmin);
+            tile_outcome(wet, bound, red, any_wet, bmin);
             if (threadIdx.x == 0) {
                 s.blk[kBlkWords * b + kBlkWet] = any_wet ? 1u : 0u;
                 if (bmin != kNoBound) atomicMin(&s.dt_buf[kDtWords * inst + 1], bmin);
@@ -383,7 +383,7 @@ __global__ void __launch_bounds__(kThreads, SWE_STAGED_MIN_CTAS)
         if (STAGE == 1) {
             bool any_wet;
             uint32_t bmin;
-            tile_verdicts(wet, bound, red, any_wet, bmin);
+            tile_outcome(wet, bound, red, any_wet, bmin);
             if (tid == 0) {
                 s.blk[kBlkWords * b + kBlkWet] = any_wet ? 1u : 0u;
                 if (bmin != kNoBound) atomicMin(&s.dt_buf[kDtWords * m.block_inst[b] + 1], bmin);

@@ -465,7 +465,7 @@ __device__ __forceinline__ bool tile_compute(const swe_mesh_t &m, const swe_stat
     if (STAGE == 1) {
         bool any_wet;
         uint32_t bmin;
-        tile_verdicts(wet, bound, red, any_wet, bmin);
+        tile_outcome(wet, bound, red, any_wet, bmin);
         if (tid == 0) {
             if (any_wet) s.blk[kBlkWords * b + kBlkWet] = 1u;
             if (bmin != kNoBound) atomicMin(&s.dt_buf[kDtWords * it.inst + 1], bmin);
