@@ -196,7 +196,8 @@ size_t swe_workspace_bytes(uint32_t n_blocks, uint32_t n_inst);
 
 /* Sets the shared-memory size of every per-block kernel for this mesh (call
    once, before any stream capture) and returns the persistent CTAs per SM of
-   the chosen stage kernel (swe_params_t.kernel). */
+   the chosen stage kernel (swe_params_t.kernel); for kernel 3, 0 when the mesh's
+   largest block does not fit its shared memory (the kernel then refuses to run). */
 int swe_configure(const swe_mesh_t *mesh, int kernel, int *blocks_per_sm);
 
 /* One Heun stage over the active blocks, fused: edge fluxes of each tile into
