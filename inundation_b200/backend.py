@@ -137,11 +137,12 @@ class SWESolverB200Resident(ResidentEngine):
         return buf
 
     def _download(self, name: str) -> NDArray[np.float32]:
-        buf = self._staging("down")
+        # straight into a new host array: one copy (measured faster than a page-locked
+        # staging buffer followed by a host copy into the array the caller keeps)
+        out = np.empty(self.N, np.float32)
         with torch.cuda.stream(self._stream):
-            buf.copy_(self._t[name][: self.N], non_blocking=True)
-        self._stream.synchronize()
-        return buf.numpy().copy()
+            torch.from_numpy(out).copy_(self._t[name][: self.N])
+        return out
 
     def download_h(self) -> NDArray[np.float32]:
         return self._download("h")

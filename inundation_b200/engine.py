@@ -341,9 +341,8 @@ class ResidentEngine:
         return slice(off, off + int(self.layout.inst_cells[inst]))
 
     def download_state(self, name: str, inst: int = 0) -> NDArray[np.float32]:
-        with torch.cuda.stream(self._stream):
-            out = self._t[name][self._inst_range(inst)].cpu().numpy()
-        return out.copy()
+        with torch.cuda.stream(self._stream):  # a new host array, written by the copy itself
+            return self._t[name][self._inst_range(inst)].cpu().numpy()
 
     def upload_state(self, name: str, values: NDArray[np.float32], inst: int = 0) -> None:
         src = torch.from_numpy(np.ascontiguousarray(values, np.float32).ravel())
