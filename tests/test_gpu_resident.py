@@ -87,6 +87,18 @@ def test_stage_kernels_agree_bit_for_bit(other: str, grid) -> None:
     assert_identical(a, b, run(a, t_end, source_rate=src), run(b, t_end, source_rate=src))
 
 
+@pytest.mark.parametrize("case", ["wetting", "dam_break", "draining"])
+@pytest.mark.parametrize("ctas", [3, 5])
+def test_persistent_kernel_on_a_few_ctas_agrees_bit_for_bit(case: str, ctas: int, grid) -> None:
+    """The 32 tiles of the valley on 3 or 5 CTAs: each CTA computes its seat, keeps one other tile
+    from step to step and takes the rest from the queue, while tiles wet, dry and change hands."""
+    h0, src, t_end = cases(grid)[case]
+    a = make(grid, h0, stage_kernel="tiled")
+    b = make(grid, h0, stage_kernel="persistent", max_grid=ctas)
+    assert b.grid(2) == ctas
+    assert_identical(a, b, run(a, t_end, source_rate=src), run(b, t_end, source_rate=src))
+
+
 # -- active set ---------------------------------------------------------------------------------------
 def same_on_off(on, off, snaps_on, snaps_off) -> None:
     assert on.steps_total == off.steps_total and len(snaps_on) == len(snaps_off)
