@@ -117,6 +117,26 @@ def test_ctypes_structs_match_the_header_layout() -> None:
 
 
 @pytest.mark.parametrize("name", ["voronoi", "valley", "mixed"])
+def test_tile_segments_put_the_records_that_read_other_tiles_last(name: str) -> None:
+    """Per segment: edges with both cells in the tile (or a wall), then the tile's edges to other
+    tiles, then the edges whose left cell is outside; each group in resident order."""
+    offsets = GEO[f"{name}_in_offsets"]
+    raw = build_geometry(GEO[f"{name}_in_verts"], GEO[f"{name}_in_faces"], offsets if offsets.size else None,
+                         zb_from_file=GEO[f"{name}_in_zb"])
+    layout = build_tile_layout(hilbert_reorder(raw, verbose=False)[0])
+    for T in (layout.blocks, layout.subs):
+        for t in range(T.n_tiles):
+            r = slice(int(T.ptr[t]), int(T.ptr[t]) + int(T.count[t]))
+            left_in = T.cl[r] // T.tile_cells == t
+            right_in = (T.cr[r] < 0) | (T.cr[r] // T.tile_cells == t)
+            group = np.where(left_in & right_in, 0, np.where(left_in, 1, 2))
+            assert (np.diff(group) >= 0).all()
+            edge = T.edge[r]
+            for k in range(3):
+                assert (np.diff(edge[group == k]) > 0).all()  # resident order within each group
+
+
+@pytest.mark.parametrize("name", ["voronoi", "valley", "mixed"])
 def test_tile_layout_resolves_every_csr_slot(name: str) -> None:
     offsets = GEO[f"{name}_in_offsets"]
     raw = build_geometry(GEO[f"{name}_in_verts"], GEO[f"{name}_in_faces"], offsets if offsets.size else None,
