@@ -86,6 +86,8 @@ def solver_of(sc, kinds, values, kernel: str = "tiled"):
 
     s = SWESolverB200Resident(sc.geom, None, sc.h0, sc.hu0, sc.hv0, sc.manning, dry_tol=DRY_TOL,
                               open_edges=sc.meta["open_edges"])
+    if kernel == "persistent-3ctas":  # 94 tiles on 3 CTAs: seats, kept tiles and the queue
+        kernel, s.max_grid = "persistent", 3
     s.stage_kernel = kernel
     s.steps_per_graph = 20
     s.set_open_conditions(kinds, values)
@@ -113,7 +115,7 @@ def oracles():
     return out
 
 
-@pytest.mark.parametrize("kernel", ["tiled", "plain", "staged", "persistent"])
+@pytest.mark.parametrize("kernel", ["tiled", "plain", "staged", "persistent", "persistent-3ctas"])
 @pytest.mark.parametrize("case", list(CASES))
 def test_runs_match_the_oracle_bit_for_bit(case: str, kernel: str, oracles) -> None:
     sc, kinds, values, t_end = channel(case)
