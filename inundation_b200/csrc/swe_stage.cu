@@ -20,29 +20,16 @@
 
 namespace swe {
 
-// Per-edge words of a tile in shared memory (also used by the prologue).
-struct TileSmem {
-    float *F0, *L1, *L2, *R1, *R2, *C;
-    uint8_t *live;
-};
-
-__device__ __forceinline__ TileSmem tile_smem(uint32_t cap) {
+// A block's edge words in shared memory: the six side words, then the CFL word.
+__device__ __forceinline__ SideWords block_side_words(uint32_t cap) {
     extern __shared__ float4 smem4[];
     float *f = reinterpret_cast<float *>(smem4);
-    TileSmem t;
-    t.F0 = f;
-    t.L1 = f + cap;
-    t.L2 = f + 2 * cap;
-    t.R1 = f + 3 * cap;
-    t.R2 = f + 4 * cap;
-    t.C = f + 5 * cap;
-    t.live = reinterpret_cast<uint8_t *>(f + 6 * cap);
-    return t;
+    return SideWords{f, f + 6 * cap, cap};
 }
 
 inline size_t block_smem_bytes(uint32_t max_tile_edges) {
     const size_t cap = (max_tile_edges + 3u) & ~3u;
-    return cap * 6 * sizeof(float) + ((cap + 15) & ~size_t(15));
+    return cap * 7 * sizeof(float);
 }
 
 // ---------------------------------------------------------------------------
@@ -62,7 +49,7 @@ template <int STAGE, bool COMP, bool CLAMP, bool OPEN>
 __global__ void __launch_bounds__(kThreads, SWE_BLOCK_MIN_CTAS)
     stage_block_kernel(swe_mesh_t m, swe_state_t s, Phys p, float cfl, float *sums) {
     const uint32_t cap = (m.max_tile_edges + 3u) & ~3u;
-    const TileSmem t = tile_smem(cap);
+    const SideWords S = block_side_words(cap);
     __shared__ uint32_t red[2 * kThreads / 32];
     const uint32_t count = s.sched[kSchedActive];
     uint64_t computed = 0;
@@ -94,13 +81,13 @@ __global__ void __launch_bounds__(kThreads, SWE_BLOCK_MIN_CTAS)
                 load_state<STAGE>(s, cR, hR, huR, hvR);
             }
             const bool live = !(hL < p.dry_tol && hR < p.dry_tol) || (OPEN && open_forced(kind, value));
-            t.live[j] = live;
-            if (!live) continue;
-            float c;
-            edge_words<OPEN>(p, cR, nx, ny, m.tile_len[e], m.tile_dzl[e], m.tile_dzr[e], hL, huL, hvL, hR, huR, hvR,
-                       t.F0[j], t.L1[j], t.L2[j], t.R1[j], t.R2[j], c, kind, value);
-            if (STAGE == 1) t.C[j] = c;
-            if (OPEN && cR < -1) tally_open(s.open_vol, static_cast<uint32_t>(-2 - cR), (0.5f * dt) * t.F0[j]);
+            float w0 = 0.0f, w1 = 0.0f, w2 = 0.0f, w3 = 0.0f, w4 = 0.0f, w5 = 0.0f;
+            if (live) {
+                edge_words<OPEN>(p, cR, nx, ny, m.tile_len[e], m.tile_dzl[e], m.tile_dzr[e], hL, huL, hvL, hR, huR,
+                                 hvR, w0, w1, w2, w3, w4, w5, kind, value);
+                if (OPEN && cR < -1) tally_open(s.open_vol, static_cast<uint32_t>(-2 - cR), (0.5f * dt) * w0);
+            }
+            put_side_words<STAGE>(S, j, live, w0, w1, w2, w3, w4, w5);
         }
         __syncthreads();
 
@@ -109,21 +96,8 @@ __global__ void __launch_bounds__(kThreads, SWE_BLOCK_MIN_CTAS)
         uint32_t bound = kNoBound;
         if (threadIdx.x < cells) {
             float sdh = 0.0f, sdhu = 0.0f, sdhv = 0.0f, lam = 0.0f;
-            for (uint32_t k = m.cptr[i], k1 = m.cptr[i + 1]; k < k1; ++k) {
-                const uint32_t v = m.lcsr[k];
-                const uint32_t j = v >> 1;
-                if (!t.live[j]) continue;  // a dry-dry edge was not computed and adds nothing
-                if (v & 1u) {
-                    sdh -= t.F0[j];
-                    sdhu -= t.R1[j];
-                    sdhv -= t.R2[j];
-                } else {
-                    sdh += t.F0[j];
-                    sdhu += t.L1[j];
-                    sdhv += t.L2[j];
-                }
-                if (STAGE == 1) lam += t.C[j];
-            }
+            for (uint32_t k = m.cptr[i], k1 = m.cptr[i + 1]; k < k1; ++k)
+                add_side_words<STAGE>(S, m.lcsr[k], sdh, sdhu, sdhv, lam);
             const float hi = STAGE ? s.h1[i] : s.h[i], hui = STAGE ? s.hu1[i] : s.hu[i];
             const float hvi = STAGE ? s.hv1[i] : s.hv[i];
             const float loi = COMP ? (STAGE ? s.h1_lo[i] : s.h_lo[i]) : 0.0f;
@@ -217,10 +191,8 @@ __global__ void __launch_bounds__(kThreads, SWE_STAGED_MIN_CTAS)
     float *C = Rdzr + L.capE;  // columns: 0..3 the stage's input state, 4 area, 5 n, 6..9 committed
     uint32_t *Cp = reinterpret_cast<uint32_t *>(C + nc * kBlockCells);
     uint16_t *Lc = reinterpret_cast<uint16_t *>(Cp + 260);
-    // The flux words overwrite the records: live flag over cR, words 0..4 over nx..dzr, CFL word over cL.
-    int32_t *live_w = Rcr;
-    float *W0 = Rnx, *W1 = Rny, *W2 = Rlen, *W3 = Rdzl, *W4 = Rdzr;
-    int32_t *W5 = Rcl;
+    // The flux words overwrite the records: the six side words over cR..dzr, the CFL word over cL.
+    const SideWords S{reinterpret_cast<float *>(Rcr), reinterpret_cast<float *>(Rcl), L.capE};
     const uint32_t tid = threadIdx.x;
     const uint32_t count = s.sched[kSchedActive];
     if (tid == 0) {
@@ -326,18 +298,13 @@ __global__ void __launch_bounds__(kThreads, SWE_STAGED_MIN_CTAS)
             }
             const bool live = !(hL < p.dry_tol && hR < p.dry_tol) || (OPEN && open_forced(kind, value));
             const float len = Rlen[j], dzl = Rdzl[j], dzr = Rdzr[j];
-            live_w[j] = live ? 1 : 0;
-            if (!live) continue;
-            float w0, w1, w2, w3, w4, w5;
-            edge_words<OPEN>(p, cR, nx, ny, len, dzl, dzr, hL, huL, hvL, hR, huR, hvR, w0, w1, w2, w3, w4, w5,
-                             kind, value);
-            if (OPEN && cR < -1) tally_open(s.open_vol, static_cast<uint32_t>(-2 - cR), (0.5f * dt) * w0);
-            W0[j] = w0;
-            W1[j] = w1;
-            W2[j] = w2;
-            W3[j] = w3;
-            W4[j] = w4;
-            if (STAGE == 1) W5[j] = __float_as_int(w5);
+            float w0 = 0.0f, w1 = 0.0f, w2 = 0.0f, w3 = 0.0f, w4 = 0.0f, w5 = 0.0f;
+            if (live) {
+                edge_words<OPEN>(p, cR, nx, ny, len, dzl, dzr, hL, huL, hvL, hR, huR, hvR, w0, w1, w2, w3, w4, w5,
+                                 kind, value);
+                if (OPEN && cR < -1) tally_open(s.open_vol, static_cast<uint32_t>(-2 - cR), (0.5f * dt) * w0);
+            }
+            put_side_words<STAGE>(S, j, live, w0, w1, w2, w3, w4, w5);
         }
         __syncthreads();
 
@@ -354,21 +321,7 @@ __global__ void __launch_bounds__(kThreads, SWE_STAGED_MIN_CTAS)
             }
             float sdh = 0.0f, sdhu = 0.0f, sdhv = 0.0f, lam = 0.0f;
             const uint32_t q0 = Cp[tid] - Cp[0], q1 = Cp[tid + 1] - Cp[0];
-            for (uint32_t q = q0; q < q1; ++q) {
-                const uint32_t v = Lc[q];
-                const uint32_t j = v >> 1;
-                if (!live_w[j]) continue;  // a dry-dry edge was not computed and adds nothing
-                if (v & 1u) {
-                    sdh -= W0[j];
-                    sdhu -= W3[j];
-                    sdhv -= W4[j];
-                } else {
-                    sdh += W0[j];
-                    sdhu += W1[j];
-                    sdhv += W2[j];
-                }
-                if (STAGE == 1) lam += __int_as_float(W5[j]);
-            }
+            for (uint32_t q = q0; q < q1; ++q) add_side_words<STAGE>(S, Lc[q], sdh, sdhu, sdhv, lam);
             if (sums) {
                 const uint32_t n = m.n_blocks * kBlockCells;
                 sums[i] = sdh;

@@ -11,6 +11,74 @@
 
 namespace swe {
 
+// The gather words of a tile's edges in shared memory, laid out so that both
+// cells of an edge add what they read: six arrays of `cap` words from P. The
+// left cell of edge j adds (P[j], P[cap + j], P[2 cap + j]) = (w0, w1, w2) to
+// its sums (sdh, sdhu, sdhv), the right cell (P[3 cap + j], P[4 cap + j],
+// P[5 cap + j]) = (-w0, -w3, -w4): adding -w is subtracting w, bit for bit. An
+// edge that is not computed (dry on both sides) holds -0.0 in all six, which
+// leaves a sum unchanged (x + -0.0 == x for every x, +0.0 included, in
+// round-to-nearest), so the gather needs no flag and no branch per slot and its
+// sums have the bits of sums that skip such edges. The corrector's CFL word w5,
+// which both cells add, sits at Lw[j] (-0.0 when not computed).
+struct SideWords {
+    float *P;
+    float *Lw;
+    uint32_t cap;
+};
+
+// Edge j's words: the computed ones when `live`, else -0.0 throughout.
+template <int STAGE>
+__device__ __forceinline__ void put_side_words(const SideWords &S, uint32_t j, bool live, float w0, float w1,
+                                               float w2, float w3, float w4, float w5) {
+    const float z = -0.0f;
+    float *P = S.P + j;
+    const uint32_t c = S.cap;
+    P[0] = live ? w0 : z;
+    P[c] = live ? w1 : z;
+    P[2u * c] = live ? w2 : z;
+    P[3u * c] = live ? -w0 : z;
+    P[4u * c] = live ? -w3 : z;
+    P[5u * c] = live ? -w4 : z;
+    if (STAGE == 1) S.Lw[j] = live ? w5 : z;
+}
+
+// Adds the words of local-CSR slot v (edge v >> 1, side v & 1) to a cell's sums.
+template <int STAGE>
+__device__ __forceinline__ void add_side_words(const SideWords &S, uint32_t v, float &sdh, float &sdhu, float &sdhv,
+                                               float &lam) {
+    const float *w = S.P + ((v >> 1) + (v & 1u) * 3u * S.cap);
+    sdh += w[0];
+    sdhu += w[S.cap];
+    sdhv += w[2u * S.cap];
+    if (STAGE == 1) lam += S.Lw[v >> 1];
+}
+
+// The same words in arrays of their own (the persistent kernel, whose staged
+// records stay from step to step): one float4 per local-CSR slot value
+// v = 2j + side, (w0, w1, w2, w5) for the left cell of edge j and
+// (-w0, -w3, -w4, w5) for the right, -0.0 throughout for an edge that is not
+// computed. The sums are those of SideWords, bit for bit, from one 16-byte
+// shared load per slot; F holds 8 words per record, 16-byte aligned.
+template <int STAGE>
+__device__ __forceinline__ void put_slot_words(float *F, uint32_t j, bool live, float w0, float w1, float w2,
+                                               float w3, float w4, float w5) {
+    const float z = -0.0f;
+    float4 *P = reinterpret_cast<float4 *>(F) + 2u * j;
+    const float c = (STAGE == 1 && live) ? w5 : z;
+    P[0] = live ? make_float4(w0, w1, w2, c) : make_float4(z, z, z, z);
+    P[1] = live ? make_float4(-w0, -w3, -w4, c) : make_float4(z, z, z, z);
+}
+
+template <int STAGE>
+__device__ __forceinline__ void add_slot_words(const float *F, uint32_t v, float &sdh, float &sdhu, float &sdhv,
+                                               float &lam) {
+    const float4 w = reinterpret_cast<const float4 *>(F)[v];
+    sdh += w.x;
+    sdhu += w.y;
+    sdhv += w.z;
+    if (STAGE == 1) lam += w.w;
+}
 
 // The compensated Heun update of one cell from its gathered sums (resident.py:354-513).
 // keep != nullptr: the new state also goes to shared memory at keep[0], keep[64],
@@ -330,16 +398,16 @@ struct LateDt {
 
 // Shared-memory bytes of a tile pass: two staged buffers, and with `keep` (the
 // persistent kernel, whose buffers keep their records from step to step) the
-// flux words in arrays of their own (7 per record).
+// flux words in arrays of their own (8 per record: two float4 slot words).
 __host__ __device__ inline size_t tiled_smem_bytes(uint32_t max_edges, uint32_t max_slots, bool keep) {
     const TilePlan L = tile_plan(max_edges, max_slots, 10u);
-    return keep ? L.total + 7u * L.capE * 4u : L.total;
+    return keep ? L.total + 8u * L.capE * 4u : L.total;
 }
 
 // Fluxes, gather and update of one staged tile. The stage's input state is in
 // columns in_col..in_col+3 of B.c (h, hu, hv, h_lo), the committed state of the
 // corrector in com_col..com_col+3. F == nullptr: the flux words overwrite the
-// consumed records; otherwise they go to F (7 x capE words) and the records stay.
+// consumed records (side words); otherwise they go to F (8 x capE words, slot words) and the records stay.
 // keep_pred: the new state also goes to columns 6..9 (predictor) or 0..3
 // (corrector). Returns, in the corrector and to warp 0, whether a cell of the tile is wet.
 // OPEN: the mesh has open edges (right cell -2 - k), with ghosts and tallies.
@@ -361,10 +429,8 @@ __device__ __forceinline__ bool tile_compute(const swe_mesh_t &m, const swe_stat
     if (STAGE == 0 && !late && (it.tile & 3u) == 0u && tid == 0) s.blk[kBlkWords * b + kBlkWet] = 0u;
     const float *C0 = B.c + in_col * kTileCells, *C1 = C0 + kTileCells, *C2 = C0 + 2 * kTileCells;
     const int base = static_cast<int>(it.tile * kTileCells);
-    int32_t *live_w = F ? reinterpret_cast<int32_t *>(F) : B.cr;
-    float *W0 = F ? F + capE : B.nx, *W1 = F ? F + 2 * capE : B.ny, *W2 = F ? F + 3 * capE : B.len;
-    float *W3 = F ? F + 4 * capE : B.dzl, *W4 = F ? F + 5 * capE : B.dzr;
-    int32_t *W5 = F ? reinterpret_cast<int32_t *>(F + 6 * capE) : B.cl;
+    // without F: the side words over the records cr..dzr (six arrays of capE words from B.cr), the CFL word over cl
+    const SideWords S{reinterpret_cast<float *>(B.cr), reinterpret_cast<float *>(B.cl), capE};
 
     // Edge fluxes.
     for (uint32_t j = tid; j < it.ne; j += TPB) {
@@ -400,18 +466,16 @@ __device__ __forceinline__ bool tile_compute(const swe_mesh_t &m, const swe_stat
         }
         const bool live = !(hL < p.dry_tol && hR < p.dry_tol) || (OPEN && open_forced(kind, value));
         const float len = B.len[j], dzl = B.dzl[j], dzr = B.dzr[j];
-        live_w[j] = live ? 1 : 0;
-        if (!live) continue;
-        float w0, w1, w2, w3, w4, w5;
-        edge_words<OPEN>(p, cR, nx, ny, len, dzl, dzr, hL, huL, hvL, hR, huR, hvR, w0, w1, w2, w3, w4, w5, kind,
-                         value);
-        if (OPEN && cR < -1) tally_open(s.open_vol, static_cast<uint32_t>(-2 - cR), (0.5f * dt) * w0);
-        W0[j] = w0;
-        W1[j] = w1;
-        W2[j] = w2;
-        W3[j] = w3;
-        W4[j] = w4;
-        if (STAGE == 1) W5[j] = __float_as_int(w5);
+        float w0 = 0.0f, w1 = 0.0f, w2 = 0.0f, w3 = 0.0f, w4 = 0.0f, w5 = 0.0f;
+        if (live) {
+            edge_words<OPEN>(p, cR, nx, ny, len, dzl, dzr, hL, huL, hvL, hR, huR, hvR, w0, w1, w2, w3, w4, w5, kind,
+                             value);
+            if (OPEN && cR < -1) tally_open(s.open_vol, static_cast<uint32_t>(-2 - cR), (0.5f * dt) * w0);
+        }
+        if (F)
+            put_slot_words<STAGE>(F, j, live, w0, w1, w2, w3, w4, w5);
+        else
+            put_side_words<STAGE>(S, j, live, w0, w1, w2, w3, w4, w5);
     }
     if (late && tid == 0) {
         const uint32_t late_dt = published_dt(s, late->dt, late->epoch, late_pair);
@@ -432,20 +496,11 @@ __device__ __forceinline__ bool tile_compute(const swe_mesh_t &m, const swe_stat
     if (tid < it.cells) {
         float sdh = 0.0f, sdhu = 0.0f, sdhv = 0.0f, lam = 0.0f;
         const uint32_t k0 = B.cptr[tid] - B.cptr[0], k1 = B.cptr[tid + 1] - B.cptr[0];
-        for (uint32_t q = k0; q < k1; ++q) {
-            const uint32_t v = B.lcsr[q];
-            const uint32_t j = v >> 1;
-            if (!live_w[j]) continue;
-            if (v & 1u) {
-                sdh -= W0[j];
-                sdhu -= W3[j];
-                sdhv -= W4[j];
-            } else {
-                sdh += W0[j];
-                sdhu += W1[j];
-                sdhv += W2[j];
-            }
-            if (STAGE == 1) lam += __int_as_float(W5[j]);
+        if (F) {
+#pragma unroll 1  // unrolled, the float4 loads in flight spill the persistent kernel's registers
+            for (uint32_t q = k0; q < k1; ++q) add_slot_words<STAGE>(F, B.lcsr[q], sdh, sdhu, sdhv, lam);
+        } else {
+            for (uint32_t q = k0; q < k1; ++q) add_side_words<STAGE>(S, B.lcsr[q], sdh, sdhu, sdhv, lam);
         }
         if (sums) {  // the record the adjoint reverses
             const uint32_t n = m.n_blocks * kBlockCells, i = base + tid;
